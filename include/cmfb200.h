@@ -1,0 +1,281 @@
+/*
+ * cmfb200.h -- C ABI of libcmfb200.so, the B200 (sm_100a) river-routing core.
+ *
+ * This library replaces the per-sub-step routing path of CaMa-Flood-GPU: the
+ * native launchers in cmfgpu/phys/cuda/*.cu (bound there through hydroforge's
+ * CudaExtensionGroup, cmfgpu/phys/cuda/__init__.py:68-166).  Instead of one
+ * at::Tensor launcher per physics phase, a caller describes all model tensors
+ * once in a CmfView (plain device pointers + sizes), creates a plan, and then
+ * advances whole forcing intervals.  Per-phase entry points remain for parity
+ * work.  No torch type crosses this boundary.
+ *
+ * Ownership: every buffer in CmfView is owned by the caller.  The library never
+ * allocates device memory on the step path; cmf_plan_create allocates only the
+ * plan object (host) and, lazily, its CUDA graph.  Scratch lives in the
+ * caller-provided workspace (size from cmf_workspace_size).
+ *
+ * Errors: every entry point returns an int status (CMF_OK == 0).  Kernels
+ * report numeric trouble through the device status word (CmfView.status).
+ * Nothing aborts the process.
+ *
+ * Threading: one host thread per plan.  All work is enqueued on the caller's
+ * stream.
+ */
+#ifndef CMFB200_H
+#define CMFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMF_ABI_VERSION 1
+
+/* ---- return codes ------------------------------------------------------- */
+#define CMF_OK 0
+#define CMF_ERR_ARG 1         /* invalid argument / inconsistent view       */
+#define CMF_ERR_CUDA 2        /* a CUDA runtime call failed                  */
+#define CMF_ERR_TIMEOUT 3     /* a bounded device wait gave up               */
+#define CMF_ERR_NUMERIC 4     /* device status word reported a bad value     */
+#define CMF_ERR_UNSUPPORTED 5 /* feature combination not compiled            */
+
+/* ---- device status word bits (CmfView.status[0]) ------------------------- */
+#define CMF_STATUS_NONFINITE 1   /* NaN/Inf storage or discharge produced     */
+#define CMF_STATUS_SUBSTEP_CAP 2 /* CFL asked for more sub-steps than allowed */
+
+/* ---- feature bits (CmfView.features) ------------------------------------- */
+#define CMF_FEAT_BIFURCATION 1 /* bifurcation module open                    */
+#define CMF_FEAT_LEVEE 2       /* levee module open                          */
+#define CMF_FEAT_RESERVOIR 4   /* reservoir module open                      */
+#define CMF_FEAT_ADAPTIVE 8    /* adaptive_time module open (CFL sub-steps)  */
+#define CMF_FEAT_BUDGET 16     /* accumulate the fp64 water budget           */
+#define CMF_FEAT_FP64 32       /* REAL fields are double (else float)        */
+#define CMF_FEAT_GRAPH 64      /* run intervals through a CUDA graph         */
+
+/* ---- per-catchment flag bits (CmfView.cell_flags) ------------------------ */
+#define CMF_CELL_MOUTH 1
+#define CMF_CELL_LEVEE 2
+#define CMF_CELL_RESERVOIR 4
+#define CMF_CELL_DAM_UPSTREAM 8
+#define CMF_CELL_DAM_RELATED 16
+#define CMF_CELL_BIFURCATION 32
+
+/* ---- member-batched parameter bits (CmfView.batched_mask) ---------------- */
+/* A set bit means the parameter is stored [N, M] member-innermost instead of
+ * shared [N].  State fields are always [N, M]. */
+#define CMF_BATCH_RUNOFF 1
+#define CMF_BATCH_RIVER_MANNING 2
+#define CMF_BATCH_FLOOD_MANNING 4
+#define CMF_BATCH_RIVER_WIDTH 8
+#define CMF_BATCH_RIVER_HEIGHT 16
+#define CMF_BATCH_RIVER_LENGTH 32
+
+/* ---- fp64 water budget terms (CmfView.budget) ----------------------------- */
+#define CMF_BUDGET_STORAGE_START 0 /* sum of storage at interval start (m3)  */
+#define CMF_BUDGET_STORAGE_END 1   /* sum of storage at interval end (m3)    */
+#define CMF_BUDGET_RUNOFF_IN 2     /* runoff volume added (m3)               */
+#define CMF_BUDGET_MOUTH_OUT 3     /* volume leaving through mouths (m3)     */
+#define CMF_BUDGET_CLIP_GAIN 4     /* volume created by clipping at zero     */
+#define CMF_BUDGET_SUBSTEPS 5      /* sub-steps accumulated                  */
+#define CMF_BUDGET_TERMS 6
+
+/*
+ * CmfView: every tensor of the model, by the reference's field names.
+ * REAL pointers are float* unless CMF_FEAT_FP64 is set; STO pointers are
+ * always double* (the reference "hpfloat" storage dtype).  Catchment-indexed
+ * arrays are in the plan's catchment order, which MUST be the breadth-first
+ * order produced by cmf_topo_bfs_order (upstream cells of p are
+ * [upstream_ptr[p], upstream_ptr[p+1])).  With M > 1 members every state
+ * field is [N, M] with the member index innermost.
+ * Field order is part of the ABI; cmf_view_field_offsets() reports it.
+ */
+typedef struct CmfView {
+    int32_t abi_version;
+    int32_t features;
+    int64_t num_catchments;          /* N */
+    int32_t num_members;             /* M, 1 for the plain model */
+    int32_t num_flood_levels;        /* K, columns of flood_depth_table */
+    int64_t num_bifurcation_paths;   /* P */
+    int32_t num_bifurcation_levels;  /* L */
+    int32_t batched_mask;            /* CMF_BATCH_* bits */
+    int64_t num_levees;
+    int64_t num_reservoirs;
+    double gravity;                  /* base.gravity (9.8) */
+    double min_kinematic_slope;      /* base.min_kinematic_slope (1e-5) */
+    double adaptive_time_factor;     /* adaptive_time.adaptive_time_factor */
+    double max_sub_step_seconds;     /* optional dt cap, 0 = none */
+    int32_t max_sub_steps_cap;       /* reject intervals needing more; 0 = none */
+    int32_t block_size;              /* threads per CTA (autotuned), 0 = default */
+
+    /* topology (device, int32 / uint8) */
+    const int32_t* downstream_idx;   /* [N], self at mouths */
+    const int32_t* upstream_ptr;     /* [N+1] */
+    const uint8_t* cell_flags;       /* [N] CMF_CELL_* */
+    const int32_t* levee_slot;       /* [N] levee index or -1 */
+    const int32_t* reservoir_slot;   /* [N] reservoir index or -1 */
+    const int32_t* bif_cell_ptr;     /* [N+1] incident-path CSR */
+    const int32_t* bif_cell_paths;   /* [2P] 2*path + (cell is downstream end) */
+
+    /* base parameters (REAL, [N] or [N,M] by batched_mask) */
+    const void* river_width;
+    const void* river_length;
+    const void* river_height;
+    const void* catchment_elevation;
+    const void* catchment_area;
+    const void* downstream_distance;
+    const void* river_manning;
+    const void* flood_manning;
+    const void* flood_depth_table;   /* [N, K] row-major */
+    const void* runoff;              /* m3/s */
+
+    /* base state (REAL) */
+    void* river_outflow;
+    void* flood_outflow;
+    void* river_depth;
+    void* flood_depth;
+    void* protected_depth;
+    void* river_cross_section_depth;
+    void* flood_cross_section_depth;
+    void* flood_cross_section_area;
+    void* flood_fraction;
+    /* base state (STO = double) */
+    double* river_storage;
+    double* flood_storage;
+    double* protected_storage;
+
+    /* diagnostics written on the last sub-step of an interval (optional) */
+    double* river_inflow;
+    double* flood_inflow;
+    double* outgoing_storage;
+    double* total_storage;
+    double* global_bifurcation_outflow;
+    void* limit_rate;
+    void* water_surface_elevation;
+    void* protected_water_surface_elevation;
+
+    /* bifurcation module */
+    const int32_t* bifurcation_catchment_idx;   /* [P] */
+    const int32_t* bifurcation_downstream_idx;  /* [P] */
+    const void* bifurcation_manning;            /* [P, L] */
+    const void* bifurcation_width;              /* [P, L] */
+    const void* bifurcation_length;             /* [P] */
+    const void* bifurcation_elevation;          /* [P, L] */
+    void* bifurcation_outflow;                  /* [P, L] (x M) */
+    void* bifurcation_cross_section_depth;      /* [P, L] (x M) */
+
+    /* levee module (per levee, [Lv]) */
+    const int32_t* levee_catchment_idx;
+    const void* levee_crown_height;
+    const void* levee_fraction;
+    const void* levee_base_height;
+
+    /* reservoir module (per reservoir, [R]) */
+    const int32_t* reservoir_catchment_idx;
+    const void* conservation_volume;
+    const void* emergency_volume;
+    const void* adjustment_volume;
+    const void* effective_normal_outflow;
+    const void* adjustment_outflow;
+    const void* flood_control_outflow;
+    double* reservoir_total_inflow;             /* [N] (x M) */
+
+    /* time control (device) */
+    void* time_step;                 /* [M] REAL sub-step length */
+    void* outer_time_step;           /* [1] REAL forcing interval */
+    int32_t* max_sub_steps;          /* [M] sub-step count of the interval */
+    int32_t* current_step;           /* [1] */
+
+    /* fp64 water budget, accumulated (optional, CMF_BUDGET_TERMS x M) */
+    double* budget;
+    /* device status word (CMF_STATUS_* bits), [1] */
+    int32_t* status;
+
+    /* caller-provided scratch */
+    void* workspace;
+    size_t workspace_bytes;
+} CmfView;
+
+typedef struct CmfPlan CmfPlan;
+
+/* ---- library / ABI introspection ----------------------------------------- */
+int cmf_abi_version(void);
+const char* cmf_status_string(int code);
+/* Byte offsets of every CmfView field in declaration order; returns the
+ * number of fields (writes at most cap entries). */
+int cmf_view_field_offsets(int64_t* offsets, int cap);
+size_t cmf_view_size(void);
+
+/* ---- plan lifecycle ------------------------------------------------------ */
+/* Bytes of scratch the view needs (Qu fluxes, path sums, budget partials). */
+int cmf_workspace_size(const CmfView* view, size_t* bytes);
+/* Validate the view and bind a plan to its pointers (cmfgpu phys dispatch:
+ * BackendRegistry(...).selected binding by parameter name,
+ * cmfgpu/phys/outflow.py:51-60). */
+int cmf_plan_create(const CmfView* view, CmfPlan** plan);
+void cmf_plan_destroy(CmfPlan* plan);
+
+/* ---- the step path ------------------------------------------------------- */
+/* Advance one forcing interval of `outer_seconds`.  Replaces the body of
+ * CaMaFlood.step_advance (cmfgpu/models/cama_flood_model.py:104-173):
+ * adaptive sub-step count on the device (no host sync), dt = T / n, then n
+ * sub-steps of momentum -> limiter/inflow/stage.  fixed_sub_steps > 0 skips
+ * the CFL and uses that count (the reference's fixed mode). */
+int cmf_step_interval(CmfPlan* plan, void* stream, double outer_seconds,
+                      int32_t fixed_sub_steps);
+
+/* ---- per-phase entry points (parity / debugging) ------------------------- */
+/* Momentum phase of one sub-step.  Replaces, fused:
+ *   launch_outflow            cmfgpu/phys/cuda/outflow.cu:272-367
+ *   launch_reservoir_outflow  cmfgpu/phys/cuda/reservoir.cu:327-363
+ *   launch_bif_outflow        cmfgpu/phys/cuda/bifurcation.cu:158-199
+ *   launch_levee_bif_outflow  cmfgpu/phys/cuda/levee.cu:424-466
+ * Writes the unlimited fluxes to the workspace and the cross-section state in
+ * place.  diag != 0 also writes water_surface_elevation,
+ * protected_water_surface_elevation and total_storage. */
+int cmf_phase_momentum(CmfPlan* plan, void* stream, int diag);
+/* Limiter + inflow + storage/stage phase of one sub-step.  Replaces, fused:
+ *   launch_inflow             cmfgpu/phys/cuda/outflow.cu:389-422
+ *   launch_bif_inflow         cmfgpu/phys/cuda/bifurcation.cu:201-231
+ *   launch_flood_stage(_log)  cmfgpu/phys/cuda/storage.cu:318-445
+ *   launch_levee_stage(_log)  cmfgpu/phys/cuda/levee.cu:343-422
+ * The upstream inflow is a deterministic gather over upstream_ptr instead of
+ * fp64 atomics.  diag != 0 also writes river_inflow, flood_inflow,
+ * limit_rate, global_bifurcation_outflow and protected_depth of non-levee
+ * cells. */
+int cmf_phase_stage(CmfPlan* plan, void* stream, int diag);
+/* Adaptive sub-step count and dt for an interval of outer_seconds.  Replaces
+ *   launch_adaptive_time      cmfgpu/phys/cuda/adaptive_time.cu:50-77
+ * Writes max_sub_steps[m], time_step[m] and outer_time_step. */
+int cmf_phase_cfl(CmfPlan* plan, void* stream, double outer_seconds);
+/* Set time_step[m] = outer/n and max_sub_steps[m] = n for a fixed count. */
+int cmf_phase_fixed_dt(CmfPlan* plan, void* stream, double outer_seconds,
+                       int32_t n);
+/* Reduce the per-CTA budget partials into view.budget and clear them. */
+int cmf_budget_flush(CmfPlan* plan, void* stream);
+
+/* ---- host topology helpers (bit-exact with the reference preprocessing) -- */
+/* cmfgpu/params/utils.py:83-138 */
+int cmf_topo_topological_sort(int64_t n, const int64_t* catchment_id,
+                              const int64_t* downstream_id, int32_t* order_out);
+/* cmfgpu/params/utils.py:160-206 */
+int cmf_topo_upstream_csr(int64_t n, const int32_t* dn, int32_t* indptr,
+                          int32_t* indices);
+/* breadth-first order from the mouths (no reference counterpart) */
+int cmf_topo_bfs_order(int64_t n, const int32_t* dn, int32_t* order_out,
+                       int32_t* up_ptr_out);
+/* cmfgpu/params/utils.py:140-157 */
+int cmf_topo_init_river_depth(int64_t n, const float* catchment_elevation,
+                              const float* river_height, const int32_t* dn,
+                              const int32_t* visit, float* river_depth);
+int cmf_topo_accumulate_upstream(int64_t n, const int32_t* dn,
+                                 const double* vals, double* out);
+int cmf_topo_accumulate_downstream(int64_t n, const int32_t* dn,
+                                   const double* vals, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CMFB200_H */
