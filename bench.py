@@ -1,0 +1,402 @@
+"""Benchmark: catchment-sub-steps/s of the CaMa-Flood routing path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload full_6m|full_250k|plain_60k]
+
+A step is one forcing interval (`CaMaFlood.step_advance`, hourly for the
+default 6M-catchment full-physics workload): the CFL sub-step count, then n
+sub-steps of momentum -> limiter/inflow/stage, all in one CUDA graph launch.
+
+Printed JSON (rank 0, one line):
+  value       catchment-sub-steps/s with forcing already resident in HBM
+              (sum over ranks of N x sub-steps, / max-over-ranks device time)
+  e2e         the same metric through the public API with host buffers: every
+              step copies its runoff from pinned host memory and reads gauge
+              discharge back to the host, both inside the timed region
+  roofline    algorithmic bytes of one sub-step (momentum + stage kernels),
+              timed per kernel with CUDA events on the launch stream, against
+              the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle port timed on this host's cores (bounded sample)
+
+`--impl reference` times the reference algorithm's CPU restatement (the oracle
+port: the reference ships no CPU path) on all host cores for the same workload.
+Multi-GPU (torchrun): every rank routes its own set of basins (an independent
+network of the same size; weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "cama-flood-gpu_b200"))
+
+METRIC = "catchment-substeps/s: fwd, fwd+adjoint, 64-member batch vs plain, same GPU"
+UNIT = "catchment-substeps/s"
+
+
+def algorithmic_bytes(n: int, n_paths: int, n_levees: int, n_res: int, full: bool) -> float:
+    """Compulsory bytes of one sub-step: every parameter read once, every state
+    read and written once, forcing read once (no intermediates).
+    Per catchment: parameters 76 (9 fp32 + 40 B flood table) + runoff 4 +
+    state read 44 + state write 48 = 172.  Full physics adds per catchment
+    protected storage (16 r+w) + protected depth (8 r+w) + levee/dam masks (3),
+    16 per levee (index, crown, fraction, base), 152 per bifurcation path
+    (12 + 5 levels x (12 read + 16 read/write)) and 44 per reservoir."""
+    b = 172.0 * n
+    if full:
+        b += 27.0 * n + 16.0 * n_levees + 152.0 * n_paths + 44.0 * n_res
+    return b
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def build_workload(name: str, seed_offset: int):
+    from cmfb200 import synthetic as syn
+    cfg = dict(syn.CONFIGS[name])
+    spec = cfg["spec"]
+    spec = syn.NetworkSpec(**{**spec.__dict__, "seed": spec.seed + seed_offset})
+    net = syn.generate(spec)
+    return net, cfg
+
+
+def runoff_series(net, cfg, count: int) -> np.ndarray:
+    """Forcing of `count` consecutive intervals (input order), float32 m^3/s."""
+    from cmfb200 import synthetic as syn
+    out = np.empty((count, net.num_catchments), dtype=np.float32)
+    if cfg["interval"] >= 86400.0:
+        for k in range(count):
+            out[k] = syn.daily_runoff(net, k)
+    else:
+        per_day = int(round(86400.0 / cfg["interval"]))
+        day = None
+        for k in range(count):
+            d, h = divmod(k, per_day)
+            if d != day:
+                daily = syn.daily_runoff(net, d)
+                prof = syn.diurnal_profile(d, seed=net.spec.seed, hours=per_day)
+                day = d
+            out[k] = daily * prof[h]
+    return out
+
+
+def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15.0):
+    """Time the CPU oracle port (all host threads) on a bounded sample."""
+    from oracle import oracle as O
+    fields = O.reference_fields(net.fields, net.opened_modules)
+    orc = O.Oracle(fields, net.opened_modules)
+    threads = O.max_threads()
+    from cmfb200 import synthetic as syn
+    orc.set_runoff(runoff_series(net, cfg, 1)[0])
+    n = orc.adaptive_sub_steps(cfg["interval"], cfg.get("max_sub_step_seconds", 0.0))
+    orc.set_time_step(cfg["interval"] / max(n, 1), cfg["interval"])
+    t0 = time.perf_counter()
+    orc.substep()
+    one = time.perf_counter() - t0
+    reps = max(1, min(200, int(target_seconds / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.substep()
+    dt = time.perf_counter() - t0
+    return {
+        "value": net.num_catchments * reps / dt,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": f"{reps} sub-steps of the {net.num_catchments}-catchment network "
+                  f"(oracle/cmf_oracle.c, OpenMP, {threads} threads), dt={cfg['interval'] / max(n, 1):.1f}s",
+    }
+
+
+def run_reference(args) -> None:
+    """CPU restatement of the reference path on all host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    net, cfg = build_workload(args.workload, 0)
+    fields = O.reference_fields(net.fields, net.opened_modules)
+    orc = O.Oracle(fields, net.opened_modules)
+    threads = O.max_threads()
+    runoff = runoff_series(net, cfg, 1)[0]
+    orc.set_runoff(runoff)
+    n = orc.adaptive_sub_steps(cfg["interval"], cfg.get("max_sub_step_seconds", 0.0))
+    orc.set_time_step(cfg["interval"] / max(n, 1), cfg["interval"])
+    # one step = a bounded sample of sub-steps of the interval
+    t0 = time.perf_counter()
+    orc.substep()
+    one = time.perf_counter() - t0
+    per_step = max(1, int(4.0 / max(one, 1e-6)))
+    per_step = min(per_step, n)
+    for _ in range(args.warmup):
+        for _ in range(per_step):
+            orc.substep()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for _ in range(per_step):
+            orc.substep()
+    el = time.perf_counter() - t0
+    value = net.num_catchments * per_step * args.steps / el
+    sample = (f"{per_step} of the interval's {n} sub-steps per step, "
+              f"{net.num_catchments}-catchment {args.workload} network, {threads} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "catchments": net.num_catchments,
+                   "interval_s": cfg["interval"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from cmfb200 import CaMaFlood, _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+
+    net, cfg = build_workload(args.workload, rank)
+    full = len(net.opened_modules) > 2
+    model = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+                      step_duration=cfg["interval"],
+                      max_sub_step_seconds=cfg.get("max_sub_step_seconds", 0.0),
+                      BLOCK_SIZE=args.block)
+    N = net.num_catchments
+    P = model.bifurcation.num_bifurcation_paths if model.bifurcation is not None else 0
+    Lv = model.levee.num_levees if model.levee is not None else 0
+    R = model.reservoir.num_reservoirs if model.reservoir is not None else 0
+    total = args.warmup + args.steps
+    forcing = runoff_series(net, cfg, total)[:, model.order]          # model order
+    host = torch.from_numpy(forcing).pin_memory()
+    dev_forcing = host.to(device)
+    counts = torch.zeros(total, dtype=torch.int32, device=device)
+
+    def sync_all():
+        torch.cuda.synchronize(device)
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (also builds the interval graph)
+    for k in range(args.warmup):
+        model.set_inputs(dev_forcing[k])
+        model.step_advance()
+    sync_all()
+
+    # ---- timed region: forcing resident in HBM --------------------------------
+    gpu_index = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            gpu_index = int(vis.split(",")[local])
+        except ValueError:
+            pass
+    sampler = ClockSampler(gpu_index)
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sync_all()
+    e0.record(stream)
+    for k in range(args.warmup, total):
+        model.set_inputs(dev_forcing[k])
+        model.step_advance()
+        counts[k].copy_(model.sub_step_counts()[0])
+    e1.record(stream)
+    sync_all()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    substeps = int(counts[args.warmup:].sum().item())
+    launches = 4 * args.steps + 2 * substeps
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    w = torch.tensor([N * substeps], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(w.item()) / (ms_max / 1e3)
+
+    # ---- per-kernel timing (one interval through direct launches) -------------
+    kern = {"momentum": [], "stage": []}
+    model.set_inputs(dev_forcing[total - 1])
+    model.compute_adaptive_time_step()
+    n_int = int(model.sub_step_counts()[0].item())
+    evs = []
+    for k in range(n_int):
+        a, b, c, d = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        a.record(stream)
+        model.launch_substep_kernel(k, _lib.PART_MOMENTUM)
+        b.record(stream)
+        model.launch_substep_kernel(k, _lib.PART_STAGE)
+        c.record(stream)
+        d.record(stream)
+        evs.append((a, b, c, d))
+    model.launch_substep_kernel(n_int, _lib.PART_END)
+    torch.cuda.synchronize(device)
+    for a, b, c, d in evs:
+        kern["momentum"].append(a.elapsed_time(b))
+        kern["stage"].append(b.elapsed_time(c))
+    t_mom = float(np.mean(kern["momentum"]))
+    t_stage = float(np.mean(kern["stage"]))
+    alg = algorithmic_bytes(N, P, Lv, R, full)
+    peak, peak_kind = measured_peak()
+    achieved = alg / ((t_mom + t_stage) / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            tj = json.loads(tfile.read_text())
+            if tj.get("workload") == args.workload:
+                traffic = tj.get("bytes_per_substep")
+        except Exception:
+            traffic = None
+
+    # ---- e2e through the public API with host buffers --------------------------
+    gauges = torch.as_tensor(np.linspace(0, N - 1, 1000).astype(np.int64), device=device)
+    out_host = torch.empty((args.steps, gauges.numel()), dtype=torch.float32).pin_memory()
+    sync_all()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    e2e_sub = torch.zeros(args.steps, dtype=torch.int32, device=device)
+    for j, k in enumerate(range(args.warmup, total)):
+        model.set_inputs(host[k])                          # pinned H2D
+        model.step_advance()
+        e2e_sub[j].copy_(model.sub_step_counts()[0])
+        out_host[j].copy_(model.base.river_outflow.index_select(0, gauges), non_blocking=True)
+        torch.cuda.current_stream(device).synchronize()  # the caller reads the result
+    h1.record(stream)
+    sync_all()
+    e2e_ms = h0.elapsed_time(h1)
+    e2e_work = N * int(e2e_sub.sum().item())
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+    w2 = torch.tensor([e2e_work], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w2, op=dist.ReduceOp.SUM)
+    e2e_value = float(w2.item()) / (float(t2.item()) / 1e3)
+    model.check_status()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(net, cfg, None)
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 flux / f64 storage", "data": "synthetic (seeded generator, no CaMa maps)",
+            "config": {"workload": args.workload, "catchments_per_gpu": N,
+                       "bifurcation_paths": P, "levees": Lv, "reservoirs": R,
+                       "interval_s": cfg["interval"], "sub_steps_timed": substeps,
+                       "parallelism": f"basin-sharded x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (state ~1 GB)", "block": args.block},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 4,
+                    "d2h_bytes_per_step": int(gauges.numel()) * 4},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind, "kernel": "sub-step (k_momentum + k_stage)",
+                         "algorithmic_bytes_per_substep": alg,
+                         "ms_momentum": t_mom, "ms_stage": t_stage},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    model.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="full_6m")
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

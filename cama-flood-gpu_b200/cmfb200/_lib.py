@@ -48,6 +48,10 @@ BATCH_RIVER_WIDTH = 8
 BATCH_RIVER_HEIGHT = 16
 BATCH_RIVER_LENGTH = 32
 
+PART_MOMENTUM = 1
+PART_STAGE = 2
+PART_END = 4
+
 BUDGET_STORAGE_START = 0
 BUDGET_STORAGE_END = 1
 BUDGET_RUNOFF_IN = 2
@@ -157,6 +161,8 @@ def lib() -> ctypes.CDLL:
     h.cmf_phase_cfl.argtypes = [_P, _P, _F64]
     h.cmf_phase_fixed_dt.restype = ctypes.c_int
     h.cmf_phase_fixed_dt.argtypes = [_P, _P, _F64, _I32]
+    h.cmf_launch_substep.restype = ctypes.c_int
+    h.cmf_launch_substep.argtypes = [_P, _P, _I32, ctypes.c_int]
     h.cmf_budget_flush.restype = ctypes.c_int
     h.cmf_budget_flush.argtypes = [_P, _P]
     for name, args in {

@@ -587,6 +587,11 @@ class CaMaFlood:
         """limiter + inflow + bifurcation inflow + storage/flood/levee stage."""
         _lib.check(_lib.lib().cmf_phase_stage(self._plan, self._stream(), int(diag)), "phase_stage")
 
+    def launch_substep_kernel(self, k: int, part: int) -> None:
+        """Launch one kernel of sub-step k directly (for per-kernel timing)."""
+        _lib.check(_lib.lib().cmf_launch_substep(self._plan, self._stream(), int(k), int(part)),
+                   "launch_substep")
+
     def flush_budget(self) -> None:
         _lib.check(_lib.lib().cmf_budget_flush(self._plan, self._stream()), "budget_flush")
 

@@ -49,7 +49,10 @@ def upstream_csr(downstream_idx: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
 
 
 def bfs_order(downstream_idx: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-    """(order, up_ptr): order[new] = old index; upstream of new p = [up_ptr[p], up_ptr[p+1])."""
+    """(order, up_ptr): order[new] = old index, basin-major breadth-first.
+
+    The upstream cells of new p are [up_ptr[p], upstream_end(p)) where the end
+    is up_ptr[p+1], one less when p+1 is a mouth (see upstream_end)."""
     dn = np.ascontiguousarray(downstream_idx, dtype=np.int32)
     n = dn.shape[0]
     order = np.empty(n, dtype=np.int32)
@@ -163,3 +166,11 @@ def bifurcation_incidence(n: int, catchment_idx: np.ndarray, downstream_idx: np.
     ptr = np.zeros(n + 1, dtype=np.int32)
     np.cumsum(counts, out=ptr[1:])
     return ptr, codes[order].astype(np.int32)
+
+
+def upstream_end(up_ptr: np.ndarray, is_mouth: np.ndarray) -> np.ndarray:
+    """End of every catchment's upstream range in the bfs_order layout."""
+    n = is_mouth.shape[0]
+    end = up_ptr[1:].astype(np.int64).copy()
+    end[:-1] -= is_mouth[1:].astype(np.int64)
+    return end

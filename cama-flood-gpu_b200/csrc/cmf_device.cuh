@@ -32,11 +32,14 @@
 namespace cmf {
 
 constexpr int kMaxBifLevels = 8;
+constexpr int kMaxFloodLevels = 16;  // floodplain table columns held in registers
+constexpr int kMaxBlock = 256;       // threads per CTA (kernels use __launch_bounds__(256))
 constexpr int kBudgetTerms = CMF_BUDGET_TERMS;
 // control words (Dev::ctl)
 constexpr int kCtlStep = 0;       // current sub-step index k
 constexpr int kCtlMaxSteps = 1;   // max over members of the sub-step count
 constexpr int kCtlBlocksDone = 2; // last-block-done counter of k_stage
+constexpr int kHardSubStepCap = 100000;  // bound of the device-side sub-step loop
 
 template <typename REAL>
 struct Dev {
@@ -72,6 +75,8 @@ struct Dev {
     const REAL *bman, *bwid, *blen, *belv;
     REAL *bout, *bcsd, *bsum, *braw;
     // levee
+    long NLV;
+    const int* lci;
     const REAL *lcrown, *lfrac, *lbase;
     // reservoir
     const REAL *rcons, *remerg, *radj, *rnout, *raout, *rfcout;
@@ -104,6 +109,16 @@ __device__ __forceinline__ REAL par(const REAL* p, int bit, int batched, long i,
 
 template <typename REAL>
 __device__ __forceinline__ REAL pow73(REAL x) { return x * x * cbrt(x); }
+
+// End of the upstream range of cell x.  In the basin-major breadth-first
+// order a basin's mouth sits right before its own upstream cells, so when
+// x + 1 is a mouth the range of x ends one position earlier.
+template <typename REAL>
+__device__ __forceinline__ int upstream_end(const Dev<REAL>& v, long x)
+{
+    const int e = v.up[x + 1];
+    return (x + 1 < v.N && (v.flags[x + 1] & CMF_CELL_MOUTH)) ? e - 1 : e;
+}
 
 // Member-active test and the per-member last-sub-step flag.
 //   kh >= 0: a host-chosen step index (per-phase entry points);
@@ -445,7 +460,7 @@ __device__ __forceinline__ REAL outgoing_of(const Dev<REAL>& v, long x, int m, R
     const int M = v.M;
     REAL pos = fmax(qr, (REAL)0.0) + fmax(qf, (REAL)0.0);
     double og = (double)(pos * ts);
-    const int c0 = v.up[x], c1 = v.up[x + 1];
+    const int c0 = v.up[x], c1 = upstream_end(v, x);
     for (int c = c0; c < c1; ++c) {
         const long cm = ix<ONE>(c, m, M);
         REAL nr = v.qur[cm], nf = v.quf[cm];
@@ -484,6 +499,28 @@ struct StageOut {
     REAL rdep, fdep, ffr;
 };
 
+// Load one floodplain-table row (K <= kMaxFloodLevels) into registers with
+// independent loads; 8-byte vector loads when the row allows it.
+template <typename REAL>
+__device__ __forceinline__ void load_row(const REAL* __restrict__ row, int nl,
+                                         REAL (&H)[kMaxFloodLevels])
+{
+    if (sizeof(REAL) == 4 && nl == 10 && ((uintptr_t)row & 7) == 0) {
+        const float2* r2 = reinterpret_cast<const float2*>(row);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            float2 x = __ldg(r2 + q);
+            H[2 * q] = (REAL)x.x;
+            H[2 * q + 1] = (REAL)x.y;
+        }
+#pragma unroll
+        for (int l = 10; l < kMaxFloodLevels; ++l) H[l] = (REAL)0;
+        return;
+    }
+#pragma unroll
+    for (int l = 0; l < kMaxFloodLevels; ++l) H[l] = l < nl ? __ldg(row + l) : (REAL)0;
+}
+
 template <typename REAL, bool ONE>
 __device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, double total_s,
                                             REAL rh, REAL rw, REAL rl, StageOut<REAL>& o)
@@ -509,22 +546,30 @@ __device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, d
     REAL prev_total_storage = river_max_storage;
     REAL prev_flood_depth = (REAL)0;
     REAL next_flood_depth = (REAL)0;
-    const REAL* row = v.tbl + i * (long)nl;
-    for (int l = 0; l < nl; ++l) {
-        REAL H_curr = row[l];
-        REAL W_curr = rw + (REAL)(l + 1) * width_increment;
-        REAL dS = rl * (REAL)0.5 * (prev_W + W_curr) * (H_curr - prev_H);
-        REAL S_curr = S_accum + dS;
-        next_flood_depth = H_curr;
-        if (total_storage > S_curr) {
-            level += 1;
-            prev_total_storage = S_curr;
-            prev_flood_depth = H_curr;
-            S_accum = S_curr;
-            prev_H = H_curr;
-            prev_W = W_curr;
-        } else {
-            break;
+    // The whole table row is loaded up front (independent loads, one memory
+    // latency) and scanned from registers; the scan stops at the first level
+    // the storage does not exceed, exactly as the reference's `break`.
+    REAL H[kMaxFloodLevels];
+    load_row(v.tbl + i * (long)nl, nl, H);
+    bool scanning = true;
+#pragma unroll
+    for (int l = 0; l < kMaxFloodLevels; ++l) {
+        if (l < nl && scanning) {
+            REAL H_curr = H[l];
+            REAL W_curr = rw + (REAL)(l + 1) * width_increment;
+            REAL dS = rl * (REAL)0.5 * (prev_W + W_curr) * (H_curr - prev_H);
+            REAL S_curr = S_accum + dS;
+            next_flood_depth = H_curr;
+            if (total_storage > S_curr) {
+                level += 1;
+                prev_total_storage = S_curr;
+                prev_flood_depth = H_curr;
+                S_accum = S_curr;
+                prev_H = H_curr;
+                prev_W = W_curr;
+            } else {
+                scanning = false;
+            }
         }
     }
     REAL prev_total_width = rw + (REAL)level * width_increment;
@@ -747,9 +792,24 @@ __device__ __forceinline__ void block_budget(double (&val)[kBudgetTerms], double
 // ---------------------------------------------------------------------------
 // k_stage: cell part
 // ---------------------------------------------------------------------------
+// Per-CTA queue of levee cells awaiting their re-partition (shared memory).
+// Levee cells are a minority scattered through every warp; queueing them and
+// processing the queue densely after a barrier keeps the heavy levee scan off
+// the other lanes and reuses the flood-stage result without a global pass.
+template <typename REAL>
+struct LeveeQueue {
+    int count;
+    int cell[kMaxBlock];
+    int member[kMaxBlock];
+    double rs[kMaxBlock], fs[kMaxBlock];
+    REAL rdep[kMaxBlock], fdep[kMaxBlock], ffr[kMaxBlock];
+    REAL rh[kMaxBlock], rw[kMaxBlock], rl[kMaxBlock];
+};
+
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
 __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, int kh,
-                                           int force_diag, double (&bud)[kBudgetTerms])
+                                           int force_diag, double (&bud)[kBudgetTerms],
+                                           LeveeQueue<REAL>* lq)
 {
     bool diag;
     if (!member_step(v.ctl, v.nsub, kh, m, force_diag, diag)) return;
@@ -779,7 +839,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     // upstream inflow: gather the limited fluxes of the upstream cells
     double rin = 0.0, fin = 0.0, rti = 0.0;
-    const int c0 = v.up[i], c1 = v.up[i + 1];
+    const int c0 = v.up[i], c1 = upstream_end(v, i);
     for (int c = c0; c < c1; ++c) {
         const long cm = ix<ONE>(c, m, M);
         const REAL cr = v.qur[cm], cf = v.quf[cm];
@@ -839,9 +899,10 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     const REAL rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, i, m, M);
     StageOut<REAL> s;
     flood_stage<REAL, ONE>(v, i, m, total_s, rh, rw, rl, s);
-    double p_new = 0.0;
-    REAL pdep_new = s.fdep;
-    if (lev_cell) levee_stage<REAL, ONE>(v, i, v.lslot[i], rh, rw, rl, s, p_new, pdep_new);
+    // Levee cells are re-partitioned afterwards by k_levee (compact over the
+    // levee list); the partition conserves r + f + p, so the budget's end
+    // storage can be taken here.
+    const double p_new = 0.0;
 
     if (BUDGET) {
         const double pre = rsto + fsto + prot;
@@ -856,16 +917,25 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     v.rout[im] = rout;
     v.fout[im] = fout;
-    rdst[im] = s.rs;
-    fdst[im] = s.fs;
-    v.rdep[im] = s.rdep;
-    v.fdep[im] = s.fdep;
-    v.ffr[im] = s.ffr;
-    if (lev_cell) {
-        v.ps[im] = p_new;
-        v.pdep[im] = pdep_new;
-    } else if (diag) {
-        v.pdep[im] = s.fdep;
+    if (LEV && lev_cell) {
+        const int q = atomicAdd(&lq->count, 1);
+        lq->cell[q] = (int)i;
+        lq->member[q] = m;
+        lq->rs[q] = s.rs;
+        lq->fs[q] = s.fs;
+        lq->rdep[q] = s.rdep;
+        lq->fdep[q] = s.fdep;
+        lq->ffr[q] = s.ffr;
+        lq->rh[q] = rh;
+        lq->rw[q] = rw;
+        lq->rl[q] = rl;
+    } else {
+        rdst[im] = s.rs;
+        fdst[im] = s.fs;
+        v.rdep[im] = s.rdep;
+        v.fdep[im] = s.fdep;
+        v.ffr[im] = s.ffr;
+        if (diag) v.pdep[im] = s.fdep;
     }
     if (res_cell) v.rti[im] = rti;
     if (diag) {
@@ -898,6 +968,25 @@ __device__ __forceinline__ void stage_path(const Dev<REAL>& v, long p, int m, in
     }
 }
 
+// Interval loop control, run by the last kernel of a sub-step: the last
+// block to finish advances the step counter (every block has read it by
+// then) and, inside the interval graph, sets the while-condition.
+__device__ __forceinline__ void advance_step(int* ctl, cudaGraphConditionalHandle h, int set_cond)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        int done = atomicAdd(&ctl[kCtlBlocksDone], 1);
+        if (done == (int)gridDim.x - 1) {
+            ctl[kCtlBlocksDone] = 0;
+            const int next = ctl[kCtlStep] + 1;
+            ctl[kCtlStep] = next;
+            __threadfence();
+            if (set_cond) cudaGraphSetConditional(h, next < ctl[kCtlMaxSteps] ? 1u : 0u);
+        }
+    }
+}
+
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
 __global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int set_cond)
@@ -910,6 +999,12 @@ __global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int fo
             stage_path<REAL, ONE, BIF>(v, p, m, kh);
         }
     } else {
+        __shared__ LeveeQueue<REAL> lq_storage;
+        LeveeQueue<REAL>* lq = LEV ? &lq_storage : nullptr;
+        if (LEV) {
+            if (threadIdx.x == 0) lq->count = 0;
+            __syncthreads();
+        }
         double bud[kBudgetTerms];
 #pragma unroll
         for (int q = 0; q < kBudgetTerms; ++q) bud[q] = 0.0;
@@ -917,26 +1012,39 @@ __global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int fo
         if (t < v.N * (long)v.M) {
             long i = ONE ? t : t / v.M;
             int m = ONE ? 0 : (int)(t - i * v.M);
-            stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud);
+            stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud, lq);
         }
         if (BUDGET) block_budget(bud, v.bpart, v.cell_blocks);
-    }
-    // Interval loop control: the last block to finish advances the step
-    // counter (every block has read it by then).
-    if (kh == -1) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            int done = atomicAdd(&v.ctl[kCtlBlocksDone], 1);
-            if (done == (int)gridDim.x - 1) {
-                v.ctl[kCtlBlocksDone] = 0;
-                const int next = v.ctl[kCtlStep] + 1;
-                v.ctl[kCtlStep] = next;
-                __threadfence();
-                if (set_cond) cudaGraphSetConditional(h, next < v.ctl[kCtlMaxSteps] ? 1u : 0u);
+        if (LEV) {
+            __syncthreads();
+            const int k = step_index(v.ctl, kh);
+            double* rdst = (k & 1) ? v.rs0 : v.rs1;
+            double* fdst = (k & 1) ? v.fs0 : v.fs1;
+            for (int q = threadIdx.x; q < lq->count; q += blockDim.x) {
+                const long ci = lq->cell[q];
+                const int m = lq->member[q];
+                const long cm = ix<ONE>(ci, m, v.M);
+                StageOut<REAL> st;
+                st.rs = lq->rs[q];
+                st.fs = lq->fs[q];
+                st.rdep = lq->rdep[q];
+                st.fdep = lq->fdep[q];
+                st.ffr = lq->ffr[q];
+                double p_new;
+                REAL pdep_new;
+                levee_stage<REAL, ONE>(v, ci, v.lslot[ci], lq->rh[q], lq->rw[q], lq->rl[q], st,
+                                       p_new, pdep_new);
+                rdst[cm] = st.rs;
+                fdst[cm] = st.fs;
+                v.ps[cm] = p_new;
+                v.rdep[cm] = st.rdep;
+                v.fdep[cm] = st.fdep;
+                v.pdep[cm] = pdep_new;
+                v.ffr[cm] = st.ffr;
             }
         }
     }
+    if (kh == -1) advance_step(v.ctl, h, set_cond);
 }
 
 // ---------------------------------------------------------------------------
@@ -1007,9 +1115,12 @@ __global__ void k_interval_plan(const Dev<REAL> v, int fixed_n, cudaGraphConditi
     for (int m = threadIdx.x; m < v.M; m += blockDim.x) {
         int n = fixed_n > 0 ? fixed_n : v.nsub[m];
         if (n < 1) n = 1;
-        if (v.max_sub_cap > 0 && n > v.max_sub_cap) {
+        // A non-finite depth makes the CFL count meaningless (NaN -> int is
+        // undefined); the hard cap keeps the device-side loop bounded.
+        const int cap = v.max_sub_cap > 0 ? v.max_sub_cap : kHardSubStepCap;
+        if (n > cap) {
             atomicOr(v.status, CMF_STATUS_SUBSTEP_CAP);
-            n = v.max_sub_cap;
+            n = cap;
         }
         v.nsub[m] = n;
         v.dt[m] = (REAL)(T / (double)n);

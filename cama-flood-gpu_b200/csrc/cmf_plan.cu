@@ -208,6 +208,8 @@ void fill_dev(CmfPlan* p, const Layout& L)
     d.bcsd = (REAL*)v.bifurcation_cross_section_depth;
     d.bsum = (REAL*)(ws + L.bsum);
     d.braw = (REAL*)(ws + L.braw);
+    d.NLV = (v.features & CMF_FEAT_LEVEE) ? (long)v.num_levees : 0;
+    d.lci = v.levee_catchment_idx;
     d.lcrown = (const REAL*)v.levee_crown_height;
     d.lfrac = (const REAL*)v.levee_fraction;
     d.lbase = (const REAL*)v.levee_base_height;
@@ -272,7 +274,8 @@ int validate(const CmfView* v)
             if (!q) return CMF_ERR_ARG;
     }
     if (v->features & CMF_FEAT_LEVEE) {
-        if (!v->levee_slot || !v->levee_crown_height || !v->levee_fraction || !v->levee_base_height)
+        if (!v->levee_slot || !v->levee_crown_height || !v->levee_fraction ||
+            !v->levee_base_height || !v->levee_catchment_idx || v->num_levees < 0)
             return CMF_ERR_ARG;
     }
     if (v->features & CMF_FEAT_RESERVOIR) {
@@ -422,6 +425,7 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
                                          cudaMemcpyDeviceToHost, s))) != CMF_OK)
         return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(s))) != CMF_OK) return rc;
+    if (nmax < 0 || nmax > kHardSubStepCap) return CMF_ERR_NUMERIC;
     const int grid = p->cell_blocks + p->path_blocks;
     for (int k = 0; k < nmax; ++k) {
         int kh = k, fd = 0;
@@ -676,6 +680,30 @@ int cmf_phase_fixed_dt(CmfPlan* p, void* stream, double outer_seconds, int32_t n
     int set = 0;
     void* args[] = {p->dev, &f, &h, &set};
     return launch(p->ks.plan, 1, 256, args, s);
+}
+
+int cmf_launch_substep(CmfPlan* p, void* stream, int32_t k, int part)
+{
+    if (!p || k < 0) return CMF_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = p->cell_blocks + p->path_blocks;
+    int kh = k, fd = 0;
+    if (part == CMF_PART_MOMENTUM) {
+        void* a1[] = {p->dev, &kh, &fd};
+        return launch(p->ks.momentum, grid, p->tpb, a1, s);
+    }
+    if (part == CMF_PART_STAGE) {
+        cudaGraphConditionalHandle h = 0;
+        int set = 0;
+        void* a2[] = {p->dev, &kh, &fd, &h, &set};
+        return launch(p->ks.stage, grid, p->tpb, a2, s);
+    }
+    if (part == CMF_PART_END) {
+        void* args[] = {p->dev};
+        return launch(p->ks.end, ceil_div((long)p->view.num_catchments * p->view.num_members, 256),
+                      256, args, s);
+    }
+    return CMF_ERR_ARG;
 }
 
 int cmf_budget_flush(CmfPlan* p, void* stream)

@@ -90,15 +90,19 @@ int cmf_topo_upstream_csr(int64_t n, const int32_t* dn, int32_t* indptr,
     return CMF_OK;
 }
 
-// Breadth-first catchment order seeded by the river mouths.
+// Basin-major breadth-first catchment order.
 //
-// order_out[new] = old index.  Mouths come first (in old index order), then
-// level by level every node's upstream cells are appended in old index order.
-// Consequences used by the device kernels:
+// order_out[new] = old index.  Mouths are taken in old index order; each
+// mouth's basin is emitted breadth-first (every node's upstream cells appended
+// in old index order) before the next mouth.  Consequences used by the device
+// kernels:
 //   * the upstream cells of new node p are exactly the new indices
-//     [up_ptr[p], up_ptr[p+1]) -- no index array is needed;
-//   * the downstream index is non-decreasing along each level, so
-//     downstream gathers of a warp touch a short monotone range.
+//     [up_ptr[p], up_ptr[p+1] - m) with m = 1 when p+1 is a mouth (a basin's
+//     mouth sits just before its own upstream cells) and 0 otherwise -- no
+//     index array is needed; up_ptr[n] = n;
+//   * parents precede their upstream cells and the downstream index is
+//     non-decreasing along a basin level, so downstream and upstream gathers
+//     of a warp touch short monotone ranges close to the warp's own cells.
 // up_ptr_out has n+1 entries and is expressed in the NEW order.
 // Returns CMF_ERR_ARG when some node is not connected to a mouth (cycle).
 int cmf_topo_bfs_order(int64_t n, const int32_t* dn, int32_t* order_out,
@@ -108,18 +112,23 @@ int cmf_topo_bfs_order(int64_t n, const int32_t* dn, int32_t* order_out,
     std::vector<int32_t> ptr((size_t)n + 1), idx((size_t)n);
     int rc = cmf_topo_upstream_csr(n, dn, ptr.data(), idx.data());
     if (rc != CMF_OK) return rc;
-    int64_t back = 0;
-    for (int64_t i = 0; i < n; ++i)
-        if (dn[i] == i || dn[i] < 0) order_out[back++] = (int32_t)i;
-    int64_t front = 0;
-    up_ptr_out[0] = (int32_t)back;  // the first upstream cell follows the mouths
-    while (front < back) {
-        int32_t u = order_out[front];
-        int32_t c0 = ptr[(size_t)u], c1 = ptr[(size_t)u + 1];
-        up_ptr_out[front + 1] = (int32_t)(back + (c1 - c0));
-        for (int32_t k = c0; k < c1; ++k) order_out[back++] = idx[(size_t)k];
-        ++front;
+    // Basin-major: each basin (the tree of one mouth) is laid out completely,
+    // breadth-first, before the next one starts.  Upstream ranges stay
+    // contiguous and monotone, and parent/child distances are bounded by the
+    // width of one basin's level instead of the whole network's.
+    int64_t back = 0, front = 0;
+    for (int64_t r = 0; r < n; ++r) {
+        if (!(dn[r] == r || dn[r] < 0)) continue;
+        order_out[back++] = (int32_t)r;
+        while (front < back) {
+            int32_t u = order_out[front];
+            int32_t c0 = ptr[(size_t)u], c1 = ptr[(size_t)u + 1];
+            up_ptr_out[front] = (int32_t)back;
+            for (int32_t k = c0; k < c1; ++k) order_out[back++] = idx[(size_t)k];
+            ++front;
+        }
     }
+    up_ptr_out[n] = (int32_t)back;
     return back == n ? CMF_OK : CMF_ERR_ARG;
 }
 

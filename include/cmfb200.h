@@ -85,9 +85,10 @@ extern "C" {
  * CmfView: every tensor of the model, by the reference's field names.
  * REAL pointers are float* unless CMF_FEAT_FP64 is set; STO pointers are
  * always double* (the reference "hpfloat" storage dtype).  Catchment-indexed
- * arrays are in the plan's catchment order, which MUST be the breadth-first
- * order produced by cmf_topo_bfs_order (upstream cells of p are
- * [upstream_ptr[p], upstream_ptr[p+1])).  With M > 1 members every state
+ * arrays are in the plan's catchment order, which MUST be the basin-major
+ * breadth-first order produced by cmf_topo_bfs_order: the upstream cells of p
+ * are [upstream_ptr[p], upstream_ptr[p+1] - m), m = 1 when p+1 is a mouth
+ * and 0 otherwise.  With M > 1 members every state
  * field is [N, M] with the member index innermost.
  * Field order is part of the ABI; cmf_view_field_offsets() reports it.
  */
@@ -252,6 +253,15 @@ int cmf_phase_cfl(CmfPlan* plan, void* stream, double outer_seconds);
 /* Set time_step[m] = outer/n and max_sub_steps[m] = n for a fixed count. */
 int cmf_phase_fixed_dt(CmfPlan* plan, void* stream, double outer_seconds,
                        int32_t n);
+/* One kernel of sub-step k of the current interval (after cmf_phase_cfl or
+ * cmf_phase_fixed_dt), launched directly on `stream` so a caller can time it
+ * with events: part = CMF_PART_MOMENTUM, CMF_PART_STAGE, or CMF_PART_END (the
+ * interval epilogue, after the last sub-step).  Running MOMENTUM and STAGE
+ * for k = 0..n-1 then END is exactly cmf_step_interval without the graph. */
+#define CMF_PART_MOMENTUM 1
+#define CMF_PART_STAGE 2
+#define CMF_PART_END 4
+int cmf_launch_substep(CmfPlan* plan, void* stream, int32_t k, int part);
 /* Reduce the per-CTA budget partials into view.budget and clear them. */
 int cmf_budget_flush(CmfPlan* plan, void* stream);
 
@@ -262,7 +272,7 @@ int cmf_topo_topological_sort(int64_t n, const int64_t* catchment_id,
 /* cmfgpu/params/utils.py:160-206 */
 int cmf_topo_upstream_csr(int64_t n, const int32_t* dn, int32_t* indptr,
                           int32_t* indices);
-/* breadth-first order from the mouths (no reference counterpart) */
+/* basin-major breadth-first order from the mouths (no reference counterpart) */
 int cmf_topo_bfs_order(int64_t n, const int32_t* dn, int32_t* order_out,
                        int32_t* up_ptr_out);
 /* cmfgpu/params/utils.py:140-157 */

@@ -27,7 +27,8 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB = HERE / "liborc.so"
+# CMF_ORACLE_FMA=1 selects the FMA-contracted build (see oracle/Makefile)
+LIB = HERE / ("liborc_fma.so" if os.environ.get("CMF_ORACLE_FMA") == "1" else "liborc.so")
 ROOT = HERE.parent
 sys.path.insert(0, str(ROOT / "cama-flood-gpu_b200"))
 
@@ -83,7 +84,8 @@ _lib = None
 def build() -> Path:
     """Compile liborc.so with the committed Makefile if it is missing or stale."""
     src = [HERE / "cmf_oracle.c", HERE / "cmf_oracle_impl.h", HERE / "Makefile"]
-    if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
+    libs = [HERE / "liborc.so", HERE / "liborc_fma.so"]
+    if any(not l.exists() or any(p.stat().st_mtime > l.stat().st_mtime for p in src) for l in libs):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
 

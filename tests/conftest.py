@@ -12,7 +12,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 PKG = ROOT / "cama-flood-gpu_b200"
-for p in (str(ROOT), str(PKG)):
+for p in (str(ROOT), str(PKG), str(ROOT / "tests")):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -1,0 +1,208 @@
+"""GPU parity of the CUDA path (through the C ABI).
+
+Two references on identical seeded inputs, from a state spun up by the oracle
+(floodplains, levees and negative flows active):
+
+* The reference's own CUDA kernels (oracle/_ref, the cmfgpu/phys/cuda sources
+  compiled unmodified for sm_100a): BIT-EXACT, every field, for one sub-step
+  and for a whole simulated day (hundreds of sub-steps).  The product gathers
+  upstream inflow deterministically where the reference scatters with fp64
+  atomics; the fp64 sums round to the same fp32 values.
+* The CPU oracle (oracle/cmf_oracle.c): it rounds every float operation once,
+  whereas nvcc contracts a*b+c into FMA (the reference kernels deviate from the
+  oracle identically), so one sub-step agrees to max rel err <= 1e-4 with
+  >= 99 % of cells within 1e-5; over a day threshold switches (wet/dry,
+  flow reversal) amplify this to <= 5e-3 on <= 1 % of cells.
+* fp64 mode against the fp64 oracle: one sub-step within 1e-12.
+"""
+import numpy as np
+import pytest
+import torch
+
+from cmfb200 import synthetic as syn
+from oracle import oracle as O, ref_cuda as RC
+
+import parity as P
+
+pytestmark = pytest.mark.gpu
+
+needs_ref = pytest.mark.skipif(not RC.available(), reason="oracle/_ref not built")
+
+
+def _spun_up(case, precision="float32", n=6000):
+    net = P.make_network(case, n=n)
+    orc = P.oracle_for(net, precision)
+    P.spin_up(net, orc, days=1)
+    return net, orc
+
+
+def _single_substep(case, precision="float32", n=6000):
+    net, orc = _spun_up(case, precision, n)
+    model = P.model_for(net, precision)
+    P.load_oracle_state(model, orc)
+    runoff = syn.daily_runoff(net, 5)
+    P.set_runoff_both(model, orc, runoff)
+    model.compute_adaptive_time_step()
+    n_model = int(model.sub_step_counts()[0].item())
+    n_orc = orc.adaptive_sub_steps(86400.0)
+    assert n_model == n_orc, (n_model, n_orc)
+    orc.set_time_step(86400.0 / n_orc)
+    assert float(model.base.time_step[0].item()) == orc.time_step
+    model.compute_momentum(diag=True)
+    model.compute_stage(diag=True)
+    orc.substep()
+    torch.cuda.synchronize()
+    return model, orc
+
+
+def _ref_from_oracle(net, orc):
+    f = O.reference_fields(net.fields, net.opened_modules)
+    st = orc.state()
+    f.update({k: st[k] for k in P.CELL_REAL + P.CELL_STO})
+    if "bifurcation" in net.opened_modules:
+        f.update({k: st[k] for k in P.PATH_FIELDS})
+    if "reservoir" in net.opened_modules:
+        f["reservoir_total_inflow"] = st["reservoir_total_inflow"]
+    return RC.RefCuda(f, net.opened_modules)
+
+
+def _assert_bit_exact(model, ref_state, diag: bool):
+    order = model.order
+    for k in P.CELL_REAL + P.CELL_STO:
+        np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(), ref_state[k][order],
+                                      err_msg=k)
+    if model.bifurcation is not None:
+        for k in P.PATH_FIELDS:
+            np.testing.assert_array_equal(getattr(model.bifurcation, k).cpu().numpy(),
+                                          ref_state[k], err_msg=k)
+    if model.reservoir is not None:
+        np.testing.assert_array_equal(model.reservoir.reservoir_total_inflow.cpu().numpy(),
+                                      ref_state["reservoir_total_inflow"][order])
+    if diag:
+        for k in ("river_inflow", "flood_inflow"):
+            np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(),
+                                          ref_state[k][order], err_msg=k)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", list(P.CASES))
+def test_single_substep_bit_exact_vs_reference_cuda(case, device):
+    net, orc = _spun_up(case)
+    ref = _ref_from_oracle(net, orc)
+    model = P.model_for(net)
+    P.load_oracle_state(model, orc)
+    r = syn.daily_runoff(net, 5)
+    ref.set_runoff(r)
+    model.set_inputs(torch.as_tensor(r[model.order]).cuda())
+    n = ref.adaptive_sub_steps(86400.0)
+    ref.t["time_step"].fill_(86400.0 / n)
+    model.compute_adaptive_time_step()
+    assert int(model.sub_step_counts()[0].item()) == n
+    ref.substep()
+    model.compute_momentum(diag=True)
+    model.compute_stage(diag=True)
+    torch.cuda.synchronize()
+    _assert_bit_exact(model, ref.state(), diag=True)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["plain", "full"])
+def test_interval_bit_exact_vs_reference_cuda(case, device):
+    net, orc = _spun_up(case)
+    ref = _ref_from_oracle(net, orc)
+    model = P.model_for(net)
+    P.load_oracle_state(model, orc)
+    r = syn.daily_runoff(net, 7)
+    ref.set_runoff(r)
+    model.set_inputs(torch.as_tensor(r[model.order]).cuda())
+    n = ref.step_advance(86400.0)
+    model.step_advance()
+    torch.cuda.synchronize()
+    assert int(model.sub_step_counts()[0].item()) == n
+    _assert_bit_exact(model, ref.state(), diag=True)
+
+
+@pytest.mark.parametrize("case", list(P.CASES))
+def test_single_substep_matches_oracle(case, device):
+    model, orc = _single_substep(case)
+    errs = P.compare(model, orc, diag=True)
+    bad = {k: v for k, v in errs.items() if v > 1e-4}
+    assert not bad, bad
+    frac = P.mismatch_fraction(model, orc, rtol=1e-5)
+    assert max(frac.values()) <= 0.01, frac
+
+
+@pytest.mark.parametrize("case", ["plain", "full"])
+def test_single_substep_fp64(case, device):
+    model, orc = _single_substep(case, "float64")
+    errs = P.compare(model, orc, diag=True)
+    bad = {k: v for k, v in errs.items() if v > 1e-12}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("case", ["plain", "full"])
+def test_interval_matches_oracle(case, device):
+    net, orc = _spun_up(case)
+    model = P.model_for(net)
+    P.load_oracle_state(model, orc)
+    runoff = syn.daily_runoff(net, 7)
+    P.set_runoff_both(model, orc, runoff)
+    model.step_advance()
+    n_orc = orc.step_advance(86400.0, adaptive=True)
+    torch.cuda.synchronize()
+    assert int(model.sub_step_counts()[0].item()) == n_orc
+    frac = P.mismatch_fraction(model, orc, rtol=1e-5)
+    errs = P.compare(model, orc, diag=False)
+    for k in ("river_storage", "flood_storage", "river_outflow", "river_depth", "flood_fraction"):
+        assert frac[k] <= 0.01, (k, frac[k], errs[k])
+        assert errs[k] <= 5e-3, (k, errs[k])
+    model.check_status()
+
+
+def test_graph_and_direct_paths_are_bitwise_equal(device):
+    net = P.make_network("full")
+    outs = []
+    for graph in (True, False):
+        m = P.model_for(net, use_cuda_graph=graph)
+        for d in range(2):
+            m.set_inputs(torch.as_tensor(m.to_model_order(syn.daily_runoff(net, d))).cuda())
+            m.step_advance()
+        torch.cuda.synchronize()
+        outs.append({k: v.cpu().numpy().copy() for k, v in m.state_tensors().items()})
+    for k in outs[0]:
+        np.testing.assert_array_equal(outs[0][k], outs[1][k], err_msg=k)
+
+
+def test_run_twice_is_deterministic(device):
+    net = P.make_network("full")
+    outs = []
+    for _ in range(2):
+        m = P.model_for(net)
+        for d in range(2):
+            m.set_inputs(torch.as_tensor(m.to_model_order(syn.daily_runoff(net, d))).cuda())
+            m.step_advance()
+        torch.cuda.synchronize()
+        outs.append({k: v.cpu().numpy().copy() for k, v in m.state_tensors().items()})
+    for k in outs[0]:
+        np.testing.assert_array_equal(outs[0][k], outs[1][k], err_msg=k)
+
+
+@pytest.mark.parametrize("case", ["plain", "full"])
+def test_water_budget_closes(case, device):
+    """fp64 budget: storage change = runoff in - mouth outflow + clip gain, to
+    1e-9 of the storage over three simulated days."""
+    net = P.make_network(case, n=20000)
+    m = P.model_for(net, budget=True)
+    total_start = None
+    for d in range(3):
+        m.set_inputs(torch.as_tensor(m.to_model_order(syn.daily_runoff(net, d))).cuda())
+        m.step_advance()
+        b = m.log.budget.cpu().numpy()
+        if total_start is None:
+            total_start = b[0]
+    b = m.log.budget.cpu().numpy()
+    s_now = float((m.base.river_storage + m.base.flood_storage + m.base.protected_storage).sum())
+    gained = b[2] - b[3] + b[4]
+    resid = (s_now - total_start) - gained
+    assert abs(resid) <= 1e-9 * s_now, (resid, s_now, b)
+    assert b[5] > 0

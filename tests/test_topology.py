@@ -75,22 +75,30 @@ def test_bfs_order_properties(n, seed):
     inv = np.empty(n, dtype=np.int64)
     inv[order] = np.arange(n)
     new_dn = inv[dn[order]]
-    # upstream cells of p are exactly [up[p], up[p+1])
+    mouth = new_dn == np.arange(n)
+    end = topology.upstream_end(up, mouth)
+    # upstream cells of p are exactly [up[p], end[p])
     for p in range(0, n, max(1, n // 500)):
-        kids = np.arange(up[p], up[p + 1])
+        kids = np.arange(up[p], end[p])
         assert np.all(new_dn[kids] == p)
         assert np.all(kids != p)
-    nm0 = int((new_dn == np.arange(n)).sum())
-    assert up[0] == nm0 and up[-1] == n
-    # mouths first; parents precede children
-    mouth = new_dn == np.arange(n)
-    nm = int(mouth.sum())
-    assert mouth[:nm].all() and not mouth[nm:].any()
+    assert up[-1] == n and np.all(np.diff(up) >= 0)
+    assert np.all(up[:-1] > np.arange(n))          # upstream cells follow their parent
+    assert np.all(end >= up[:-1])
+    assert mouth[0]
+    # parents precede children
     assert np.all(new_dn[~mouth] < np.flatnonzero(~mouth))
+    # basin-major: every basin occupies one contiguous range starting at its mouth
+    root = np.arange(n)
+    for p in range(n):
+        root[p] = p if mouth[p] else root[new_dn[p]]
+    starts = np.flatnonzero(mouth)
+    assert np.all(np.diff(root) >= 0)
+    assert np.array_equal(np.unique(root), starts)
     # the same CSR as the reference semantics, relabelled
     ptr, ind = topology.upstream_csr(new_dn.astype(np.int32))
-    np.testing.assert_array_equal(ptr, up - nm)
-    np.testing.assert_array_equal(ind, np.arange(nm, n))
+    np.testing.assert_array_equal(np.diff(ptr), end - up[:-1])
+    np.testing.assert_array_equal(ind, np.flatnonzero(~mouth))
 
 
 def test_bfs_order_rejects_cycles():
