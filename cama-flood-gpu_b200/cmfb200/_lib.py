@@ -51,6 +51,7 @@ BATCH_RIVER_LENGTH = 32
 PART_MOMENTUM = 1
 PART_STAGE = 2
 PART_END = 4
+PART_LIMIT = 8
 
 BUDGET_STORAGE_START = 0
 BUDGET_STORAGE_END = 1

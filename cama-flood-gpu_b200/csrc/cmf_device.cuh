@@ -93,6 +93,7 @@ struct Dev {
     int* status;
     // scratch fluxes
     REAL *qur, *quf;
+    REAL* lrs;  // limit rate of the current sub-step, per cell x member
 };
 
 // ---------------------------------------------------------------------------
@@ -831,11 +832,8 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     const double prot = lev_cell ? v.ps[im] : 0.0;
     const REAL qr = v.qur[im], qf = v.quf[im];
 
-    // own limit rate: outgoing = own positive flux + upstream negative fluxes
-    // (+ bifurcation ends)
-    const REAL outgoing = outgoing_of<REAL, ONE, BIF>(v, i, m, ts, qr, qf);
-    const REAL rate_storage = (REAL)(rsto + fsto);
-    const REAL lr_i = (outgoing > (REAL)1e-8) ? fmin(rate_storage / outgoing, (REAL)1.0) : (REAL)1.0;
+    // limit rates of this sub-step were computed once per cell by k_limit
+    const REAL lr_i = v.lrs[im];
 
     // upstream inflow: gather the limited fluxes of the upstream cells
     double rin = 0.0, fin = 0.0, rti = 0.0;
@@ -843,7 +841,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     for (int c = c0; c < c1; ++c) {
         const long cm = ix<ONE>(c, m, M);
         const REAL cr = v.qur[cm], cf = v.quf[cm];
-        const REAL lr_c = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, c, m, ts);
+        const REAL lr_c = v.lrs[cm];
         const REAL ur = (cr >= (REAL)0.0) ? cr * lr_c : cr * lr_i;
         const REAL uf = (cf >= (REAL)0.0) ? cf * lr_c : cf * lr_i;
         rin += (double)ur;
@@ -854,7 +852,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     // own limited flux (the downstream rate is needed only for negative flux)
     REAL lr_dn = lr_i;
     if (!mouth && (qr < (REAL)0.0 || qf < (REAL)0.0))
-        lr_dn = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, v.dn[i], m, ts);
+        lr_dn = v.lrs[ix<ONE>(v.dn[i], m, M)];
     const REAL rout = (qr >= (REAL)0.0) ? qr * lr_i : qr * lr_dn;
     const REAL fout = (qf >= (REAL)0.0) ? qf * lr_i : qf * lr_dn;
 
@@ -867,7 +865,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
             const int p = e >> 1;
             const REAL raw = v.braw[ix<ONE>(p, m, M)];
             const int other = (e & 1) ? v.bci[p] : v.bdi[p];
-            const REAL lr_o = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, other, m, ts);
+            const REAL lr_o = v.lrs[ix<ONE>(other, m, M)];
             const REAL lr_c = (e & 1) ? lr_o : lr_i;
             const REAL lr_d = (e & 1) ? lr_i : lr_o;
             const REAL net = (raw >= (REAL)0) ? raw * lr_c : raw * lr_d;
@@ -954,18 +952,35 @@ __device__ __forceinline__ void stage_path(const Dev<REAL>& v, long p, int m, in
 {
     bool diag;
     if (!member_step(v.ctl, v.nsub, kh, m, 2, diag)) return;
-    const int k = step_index(v.ctl, kh);
-    const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
-    const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
-    const REAL ts = v.dt[m];
     const int ci = v.bci[p], di = v.bdi[p];
-    const REAL lr_c = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, ci, m, ts);
-    const REAL lr_d = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, di, m, ts);
+    const REAL lr_c = v.lrs[ix<ONE>(ci, m, v.M)];
+    const REAL lr_d = v.lrs[ix<ONE>(di, m, v.M)];
     for (int lv = 0; lv < v.L; ++lv) {
         const long ls = ix<ONE>(p * (long)v.L + lv, m, v.M);
         REAL o = v.bout[ls];
         v.bout[ls] = (o >= (REAL)0) ? o * lr_c : o * lr_d;
     }
+}
+
+// ---------------------------------------------------------------------------
+// k_limit: the storage-based outflow limiter rate of every catchment
+// (outflow.cu:196-203) from this sub-step's unlimited fluxes, computed once
+// per cell; k_stage reads it for the cell, its upstream cells, its downstream
+// cell and its bifurcation partners.
+// ---------------------------------------------------------------------------
+template <typename REAL, bool ONE, bool BIF>
+__global__ void __launch_bounds__(256) k_limit(const Dev<REAL> v, int kh)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= v.N * (long)v.M) return;
+    long i = ONE ? t : t / v.M;
+    int m = ONE ? 0 : (int)(t - i * v.M);
+    bool diag;
+    if (!member_step(v.ctl, v.nsub, kh, m, 2, diag)) return;
+    const int k = step_index(v.ctl, kh);
+    const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
+    const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
+    v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
 }
 
 // Interval loop control, run by the last kernel of a sub-step: the last

@@ -35,6 +35,7 @@ struct KernelSet {
     const void* plan;
     const void* end;
     const void* copy_back;
+    const void* limit;
 };
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUD>
@@ -48,6 +49,7 @@ KernelSet make_set()
     k.plan = (const void*)k_interval_plan<REAL>;
     k.end = (const void*)k_interval_end<REAL, ONE>;
     k.copy_back = (const void*)k_copy_back<REAL, ONE>;
+    k.limit = (const void*)k_limit<REAL, ONE, BIF>;
     return k;
 }
 
@@ -80,7 +82,7 @@ KernelSet pick_one(bool one, bool res, bool lev, bool bif, bool bud)
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t qur, quf, bsum, braw, rs1, fs1, bpart, ctl, tsec, total;
+    size_t qur, quf, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec, total;
 };
 
 Layout layout_of(const CmfView* v, int cell_blocks)
@@ -91,6 +93,7 @@ Layout layout_of(const CmfView* v, int cell_blocks)
     Layout L;
     size_t o = 0;
     L.qur = o; o = align_up(o + nm * real);
+    L.lrs = o; o = align_up(o + nm * real);
     L.quf = o; o = align_up(o + nm * real);
     L.bsum = o; o = align_up(o + pm * real);
     L.braw = o; o = align_up(o + pm * real);
@@ -231,6 +234,7 @@ void fill_dev(CmfPlan* p, const Layout& L)
     d.status = v.status;
     d.qur = (REAL*)(ws + L.qur);
     d.quf = (REAL*)(ws + L.quf);
+    d.lrs = (REAL*)(ws + L.lrs);
     std::memcpy(p->dev, &d, sizeof(d));
 }
 
@@ -349,13 +353,16 @@ int build_graph(CmfPlan* p, double T, int fixed_n)
         if ((rc = check_cuda(cudaGraphAddNode(&nwhile, g, &nplan, 1, &cp))) != CMF_OK) goto fail;
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         const int grid = p->cell_blocks + p->path_blocks;
-        cudaGraphNode_t b1, b2;
+        cudaGraphNode_t b1, bl, b2;
         int kh = -1, fd = 0;
         void* a1[] = {p->dev, &kh, &fd};
         if ((rc = add_kernel(&b1, body, nullptr, 0, p->ks.momentum, grid, p->tpb, a1)) != CMF_OK) goto fail;
+        void* al[] = {p->dev, &kh};
+        if ((rc = add_kernel(&bl, body, &b1, 1, p->ks.limit, p->cell_blocks, p->tpb, al)) != CMF_OK)
+            goto fail;
         int set = 1;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
-        if ((rc = add_kernel(&b2, body, &b1, 1, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
+        if ((rc = add_kernel(&b2, body, &bl, 1, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
     }
     {
         const int eb = ceil_div((long)v.num_catchments * v.num_members, 256);
@@ -431,6 +438,8 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
         int kh = k, fd = 0;
         void* a1[] = {p->dev, &kh, &fd};
         if ((rc = launch(p->ks.momentum, grid, p->tpb, a1, s)) != CMF_OK) return rc;
+        void* al[] = {p->dev, &kh};
+        if ((rc = launch(p->ks.limit, p->cell_blocks, p->tpb, al, s)) != CMF_OK) return rc;
         cudaGraphConditionalHandle h = 0;
         int set = 0;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
@@ -634,8 +643,11 @@ int cmf_phase_stage(CmfPlan* p, void* stream, int diag)
     int kh = -2, fd = diag ? 1 : 2;
     cudaGraphConditionalHandle h = 0;
     int set = 0;
+    void* al[] = {p->dev, &kh};
+    int rc = launch(p->ks.limit, p->cell_blocks, p->tpb, al, s);
+    if (rc != CMF_OK) return rc;
     void* args[] = {p->dev, &kh, &fd, &h, &set};
-    int rc = launch(p->ks.stage, p->cell_blocks + p->path_blocks, p->tpb, args, s);
+    rc = launch(p->ks.stage, p->cell_blocks + p->path_blocks, p->tpb, args, s);
     if (rc != CMF_OK) return rc;
     void* a2[] = {p->dev};
     return launch(p->ks.copy_back,
@@ -691,6 +703,10 @@ int cmf_launch_substep(CmfPlan* p, void* stream, int32_t k, int part)
     if (part == CMF_PART_MOMENTUM) {
         void* a1[] = {p->dev, &kh, &fd};
         return launch(p->ks.momentum, grid, p->tpb, a1, s);
+    }
+    if (part == CMF_PART_LIMIT) {
+        void* al[] = {p->dev, &kh};
+        return launch(p->ks.limit, p->cell_blocks, p->tpb, al, s);
     }
     if (part == CMF_PART_STAGE) {
         cudaGraphConditionalHandle h = 0;

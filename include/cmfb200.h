@@ -255,12 +255,14 @@ int cmf_phase_fixed_dt(CmfPlan* plan, void* stream, double outer_seconds,
                        int32_t n);
 /* One kernel of sub-step k of the current interval (after cmf_phase_cfl or
  * cmf_phase_fixed_dt), launched directly on `stream` so a caller can time it
- * with events: part = CMF_PART_MOMENTUM, CMF_PART_STAGE, or CMF_PART_END (the
- * interval epilogue, after the last sub-step).  Running MOMENTUM and STAGE
- * for k = 0..n-1 then END is exactly cmf_step_interval without the graph. */
+ * with events: part = CMF_PART_MOMENTUM, CMF_PART_LIMIT (the per-cell limit
+ * rate), CMF_PART_STAGE, or CMF_PART_END (the interval epilogue, after the
+ * last sub-step).  Running MOMENTUM, LIMIT and STAGE for k = 0..n-1 then END
+ * is exactly cmf_step_interval without the graph. */
 #define CMF_PART_MOMENTUM 1
 #define CMF_PART_STAGE 2
 #define CMF_PART_END 4
+#define CMF_PART_LIMIT 8
 int cmf_launch_substep(CmfPlan* plan, void* stream, int32_t k, int part);
 /* Reduce the per-CTA budget partials into view.budget and clear them. */
 int cmf_budget_flush(CmfPlan* plan, void* stream);
