@@ -164,6 +164,8 @@ def lib() -> ctypes.CDLL:
     h.cmf_phase_fixed_dt.argtypes = [_P, _P, _F64, _I32]
     h.cmf_launch_substep.restype = ctypes.c_int
     h.cmf_launch_substep.argtypes = [_P, _P, _I32, ctypes.c_int]
+    h.cmf_substep_noalloc.restype = ctypes.c_int
+    h.cmf_substep_noalloc.argtypes = [ctypes.POINTER(CmfView), _P, ctypes.c_int]
     h.cmf_budget_flush.restype = ctypes.c_int
     h.cmf_budget_flush.argtypes = [_P, _P]
     for name, args in {

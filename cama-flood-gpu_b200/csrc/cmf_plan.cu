@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <cstddef>
+#include <mutex>
 #include <new>
 
 using namespace cmf;
@@ -737,3 +738,95 @@ int cmf_budget_flush(CmfPlan* p, void* stream)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free sub-step.
+//
+// For callers that own all device memory and may not allocate any: code that
+// runs inside a stream capture, a host framework whose memory pool hands out
+// only the model tensors, or an embedded runtime without cudaMalloc.  The
+// scratch that cmf_plan_create would take from a caller workspace lives in a
+// fixed static device array instead, sized for at most
+// kNoAllocMaxCatchments catchments, kNoAllocMaxPaths bifurcation paths and
+// one member (3 MiB, held by every GPU that loads this library until exit).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr long kNoAllocMaxCatchments = 65536;
+constexpr long kNoAllocMaxPaths = 8192;
+constexpr size_t kNoAllocScratchBytes = 3u << 20;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+// Device address of g_noalloc_scratch per device (host code may not use the
+// symbol itself as a device pointer).  Looked up once per device, with that
+// device current, on its first call.
+void* g_noalloc_addr[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+int noalloc_scratch(void** out)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CMF_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return CMF_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
+            return CMF_ERR_CUDA;
+        g_noalloc_addr[dev] = addr;
+    }
+    *out = g_noalloc_addr[dev];
+    return CMF_OK;
+}
+}  // namespace
+
+extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
+{
+    if (!view) return CMF_ERR_ARG;
+    if (view->num_members != 1 || view->num_catchments > kNoAllocMaxCatchments) return CMF_ERR_ARG;
+    if ((view->features & CMF_FEAT_BIFURCATION) && view->num_bifurcation_paths > kNoAllocMaxPaths)
+        return CMF_ERR_ARG;
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc != CMF_OK) return rc;
+    CmfView v = *view;
+    v.workspace = scratch;
+    v.workspace_bytes = kNoAllocScratchBytes;
+    if ((rc = validate(&v)) != CMF_OK) return rc;
+    size_t need = 0;
+    if ((rc = cmf_workspace_size(&v, &need)) != CMF_OK) return rc;
+    if (need > kNoAllocScratchBytes) return CMF_ERR_ARG;
+
+    // A plan on the stack: kernel set and device view, no graph.
+    CmfPlan p;
+    std::memset((void*)&p, 0, sizeof(CmfPlan));
+    p.view = v;
+    const int f = v.features;
+    p.fp64 = f & CMF_FEAT_FP64;
+    p.one = true;
+    p.tpb = block_of(&v);
+    p.cell_blocks = ceil_div((long)v.num_catchments, p.tpb);
+    p.path_blocks = (f & CMF_FEAT_BIFURCATION) ? ceil_div((long)v.num_bifurcation_paths, p.tpb) : 0;
+    const bool res = f & CMF_FEAT_RESERVOIR, lev = f & CMF_FEAT_LEVEE,
+               bif = f & CMF_FEAT_BIFURCATION, bud = f & CMF_FEAT_BUDGET;
+    Layout L = layout_of(&v, p.cell_blocks);
+    if (p.fp64) {
+        p.ks = pick_one<double>(true, res, lev, bif, bud);
+        fill_dev<double>(&p, L);
+    } else {
+        p.ks = pick_one<float>(true, res, lev, bif, bud);
+        fill_dev<float>(&p, L);
+    }
+    // The array keeps the previous call's contents: clear the control words
+    // and the budget partials, which are accumulated rather than overwritten.
+    char* ws = (char*)scratch;
+    if (cudaMemsetAsync(ws + L.bpart, 0, L.tsec + 8 - L.bpart, (cudaStream_t)stream) != cudaSuccess)
+        return CMF_ERR_CUDA;
+    if ((rc = cmf_phase_momentum(&p, stream, diag)) != CMF_OK) return rc;
+    if ((rc = cmf_phase_stage(&p, stream, diag)) != CMF_OK) return rc;
+    if (bud) rc = cmf_budget_flush(&p, stream);
+    return rc;
+}

@@ -264,6 +264,21 @@ int cmf_phase_fixed_dt(CmfPlan* plan, void* stream, double outer_seconds,
 #define CMF_PART_END 4
 #define CMF_PART_LIMIT 8
 int cmf_launch_substep(CmfPlan* plan, void* stream, int32_t k, int part);
+/* One sub-step (momentum, limit rate, stage) of a single-member view that
+ * allocates nothing.  No counterpart in the reference.  It is for callers that
+ * own all device memory and cannot call cudaMalloc -- code running inside a
+ * stream capture, or a host whose memory pool hands out only the model
+ * tensors -- so they cannot supply a workspace or create a plan.  The scratch
+ * lives in a static device array of this library (3 MiB on every GPU that
+ * loads it, held until exit), which limits the view to at most 65,536
+ * catchments, 8,192 bifurcation paths and one member; larger views return
+ * CMF_ERR_ARG.  view.workspace is ignored; view.time_step[0] must hold the
+ * sub-step length.  diag != 0 writes the diagnostic fields as
+ * cmf_phase_stage does.  The first call on a device looks up the array's
+ * device address (with that device current), so make it before any stream
+ * capture.  Every call shares the one array: calls that overlap on the GPU
+ * (two streams, two host threads) race and must be serialised by the caller. */
+int cmf_substep_noalloc(const CmfView* view, void* stream, int diag);
 /* Reduce the per-CTA budget partials into view.budget and clear them. */
 int cmf_budget_flush(CmfPlan* plan, void* stream);
 
