@@ -277,7 +277,8 @@ def run_ours(args) -> None:
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     substeps = int(counts[args.warmup:].sum().item())
-    launches = 4 * args.steps + 3 * substeps   # begin, cfl, plan, end + 3 kernels per sub-step
+    per_sub = 4 if Lv > 0 else 3                 # momentum, limit, stage (+ levee)
+    launches = 4 * args.steps + per_sub * substeps   # + begin, cfl, plan, end per interval
     t = torch.tensor([ms], dtype=torch.float64, device=device)
     w = torch.tensor([N * substeps], dtype=torch.float64, device=device)
     if world > 1:
@@ -287,13 +288,13 @@ def run_ours(args) -> None:
     value = float(w.item()) / (ms_max / 1e3)
 
     # ---- per-kernel timing (one interval through direct launches) -------------
-    kern = {"momentum": [], "limit": [], "stage": []}
+    kern = {"momentum": [], "limit": [], "stage": [], "levee": []}
     model.set_inputs(dev_forcing[total - 1])
     model.compute_adaptive_time_step()
     n_int = int(model.sub_step_counts()[0].item())
     evs = []
     for k in range(n_int):
-        a, b, c, d = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        a, b, c, d, e = (torch.cuda.Event(enable_timing=True) for _ in range(5))
         a.record(stream)
         model.launch_substep_kernel(k, _lib.PART_MOMENTUM)
         b.record(stream)
@@ -301,17 +302,21 @@ def run_ours(args) -> None:
         c.record(stream)
         model.launch_substep_kernel(k, _lib.PART_STAGE)
         d.record(stream)
-        evs.append((a, b, c, d))
+        model.launch_substep_kernel(k, _lib.PART_LEVEE)
+        e.record(stream)
+        evs.append((a, b, c, d, e))
     model.launch_substep_kernel(n_int, _lib.PART_END)
     torch.cuda.synchronize(device)
-    for a, b, c, d in evs:
+    for a, b, c, d, e in evs:
         kern["momentum"].append(a.elapsed_time(b))
         kern["limit"].append(b.elapsed_time(c))
         kern["stage"].append(c.elapsed_time(d))
+        kern["levee"].append(d.elapsed_time(e))
     t_mom = float(np.mean(kern["momentum"]))
     t_lim = float(np.mean(kern["limit"]))
     t_stage = float(np.mean(kern["stage"]))
-    t_sub = t_mom + t_lim + t_stage
+    t_lev = float(np.mean(kern["levee"]))
+    t_sub = t_mom + t_lim + t_stage + t_lev
     alg = algorithmic_bytes(N, P, Lv, R, full)
     peak, peak_kind = measured_peak()
     achieved = alg / (t_sub / 1e3) / 1e9
@@ -371,9 +376,10 @@ def run_ours(args) -> None:
                     "d2h_bytes_per_step": int(gauges.numel()) * 4},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind, "kernel": "sub-step (k_momentum + k_limit + k_stage)",
+                         "peak_kind": peak_kind, "kernel": "sub-step (k_momentum + k_limit + k_stage + k_levee)",
                          "algorithmic_bytes_per_substep": alg,
-                         "ms_momentum": t_mom, "ms_limit": t_lim, "ms_stage": t_stage},
+                         "ms_momentum": t_mom, "ms_limit": t_lim, "ms_stage": t_stage,
+                         "ms_levee": t_lev},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": launches,

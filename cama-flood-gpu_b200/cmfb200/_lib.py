@@ -52,6 +52,7 @@ PART_MOMENTUM = 1
 PART_STAGE = 2
 PART_END = 4
 PART_LIMIT = 8
+PART_LEVEE = 16
 
 BUDGET_STORAGE_START = 0
 BUDGET_STORAGE_END = 1

@@ -29,10 +29,16 @@
 #include <cuda_runtime.h>
 #include "cmfb200.h"
 
+// minimum resident CTAs of k_stage per SM (caps its registers without spills)
+#ifndef CMF_STAGE_MIN_BLOCKS
+#define CMF_STAGE_MIN_BLOCKS 4
+#endif
+
 namespace cmf {
 
 constexpr int kMaxBifLevels = 8;
-constexpr int kMaxFloodLevels = 16;  // floodplain table columns held in registers
+constexpr int kRowRegs = 10;         // floodplain levels held in registers (the CaMa layout)
+constexpr int kChildUnroll = 4;      // upstream cells gathered with independent loads
 constexpr int kMaxBlock = 256;       // threads per CTA (kernels use __launch_bounds__(256))
 constexpr int kBudgetTerms = CMF_BUDGET_TERMS;
 // control words (Dev::ctl)
@@ -141,6 +147,33 @@ __device__ __forceinline__ int step_index(const int* ctl, int kh)
     return kh >= 0 ? kh : (kh == -1 ? ctl[kCtlStep] : 0);
 }
 
+// Step index, activity and last-sub-step flag of member m (see member_step).
+// With a single member the interval loop only runs k < n, so activity needs
+// no load and nothing waits on the sub-step count except the diag flag.
+struct StepInfo {
+    int k;
+    bool active;
+    bool diag;
+};
+
+template <bool ONE>
+__device__ __forceinline__ StepInfo step_info(const int* ctl, const int* nsub, int kh, int m,
+                                              int force_diag)
+{
+    StepInfo s;
+    if (kh == -2) {
+        s.k = 0;
+        s.active = true;
+        s.diag = force_diag == 1;
+        return s;
+    }
+    s.k = kh >= 0 ? kh : ctl[kCtlStep];
+    const int nm = nsub[m];
+    s.diag = (force_diag == 1) || (force_diag == 0 && s.k == nm - 1);
+    s.active = ONE || s.k < nm;
+    return s;
+}
+
 // ---------------------------------------------------------------------------
 // k_momentum: cell part (outflow.cu:21-175, reservoir.cu:18-94)
 // ---------------------------------------------------------------------------
@@ -148,9 +181,10 @@ template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF>
 __device__ __forceinline__ void momentum_cell(const Dev<REAL>& v, long i, int m, int kh,
                                               int force_diag)
 {
-    bool diag;
-    if (!member_step(v.ctl, v.nsub, kh, m, force_diag, diag)) return;
-    const int k = step_index(v.ctl, kh);
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
+    if (!st.active) return;
+    const bool diag = st.diag;
+    const int k = st.k;
     const double* __restrict__ rsrc = (k & 1) ? v.rs1 : v.rs0;
     const double* __restrict__ fsrc = (k & 1) ? v.fs1 : v.fs0;
     const int M = v.M;
@@ -354,9 +388,9 @@ __device__ __forceinline__ void path_end_state(const Dev<REAL>& v, const double*
 template <typename REAL, bool ONE, bool RES, bool LEV>
 __device__ __forceinline__ void momentum_path(const Dev<REAL>& v, long p, int m, int kh)
 {
-    bool diag;
-    if (!member_step(v.ctl, v.nsub, kh, m, 2, diag)) return;
-    const int k = step_index(v.ctl, kh);
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
+    if (!st.active) return;
+    const int k = st.k;
     const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
     const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
     const int M = v.M;
@@ -462,11 +496,23 @@ __device__ __forceinline__ REAL outgoing_of(const Dev<REAL>& v, long x, int m, R
     REAL pos = fmax(qr, (REAL)0.0) + fmax(qf, (REAL)0.0);
     double og = (double)(pos * ts);
     const int c0 = v.up[x], c1 = upstream_end(v, x);
-    for (int c = c0; c < c1; ++c) {
-        const long cm = ix<ONE>(c, m, M);
-        REAL nr = v.qur[cm], nf = v.quf[cm];
-        REAL neg = fmin(nr, (REAL)0.0) + fmin(nf, (REAL)0.0);
-        og += (double)(-neg * ts);
+    for (int cb = c0; cb < c1; cb += kChildUnroll) {
+        REAL nr[kChildUnroll], nf[kChildUnroll];
+#pragma unroll
+        for (int j = 0; j < kChildUnroll; ++j) {
+            if (cb + j < c1) {
+                const long cm = ix<ONE>(cb + j, m, M);
+                nr[j] = v.qur[cm];
+                nf[j] = v.quf[cm];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kChildUnroll; ++j) {
+            if (cb + j < c1) {
+                REAL neg = fmin(nr[j], (REAL)0.0) + fmin(nf[j], (REAL)0.0);
+                og += (double)(-neg * ts);
+            }
+        }
     }
     if (BIF && (v.flags[x] & CMF_CELL_BIFURCATION)) {
         const int b0 = v.bptr[x], b1 = v.bptr[x + 1];
@@ -500,31 +546,41 @@ struct StageOut {
     REAL rdep, fdep, ffr;
 };
 
-// Load one floodplain-table row (K <= kMaxFloodLevels) into registers with
-// independent loads; 8-byte vector loads when the row allows it.
+// A floodplain-table row held in registers (the CaMa layout has exactly
+// kRowRegs levels; other level counts scan the row from memory) together with
+// the catchment area, both needed only by flooded cells.
 template <typename REAL>
-__device__ __forceinline__ void load_row(const REAL* __restrict__ row, int nl,
-                                         REAL (&H)[kMaxFloodLevels])
+struct TableRow {
+    REAL H[kRowRegs];
+    REAL ca;
+    bool valid;
+};
+
+// Issue the row loads (independent 8-byte loads for fp32) and the area load.
+template <typename REAL>
+__device__ __forceinline__ void load_row(const Dev<REAL>& v, long i, TableRow<REAL>& r)
 {
-    if (sizeof(REAL) == 4 && nl == 10 && ((uintptr_t)row & 7) == 0) {
+    const REAL* __restrict__ row = v.tbl + i * (long)kRowRegs;
+    if (sizeof(REAL) == 4 && ((uintptr_t)row & 7) == 0) {
         const float2* r2 = reinterpret_cast<const float2*>(row);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
+        for (int q = 0; q < kRowRegs / 2; ++q) {
             float2 x = __ldg(r2 + q);
-            H[2 * q] = (REAL)x.x;
-            H[2 * q + 1] = (REAL)x.y;
+            r.H[2 * q] = (REAL)x.x;
+            r.H[2 * q + 1] = (REAL)x.y;
         }
+    } else {
 #pragma unroll
-        for (int l = 10; l < kMaxFloodLevels; ++l) H[l] = (REAL)0;
-        return;
+        for (int l = 0; l < kRowRegs; ++l) r.H[l] = __ldg(row + l);
     }
-#pragma unroll
-    for (int l = 0; l < kMaxFloodLevels; ++l) H[l] = l < nl ? __ldg(row + l) : (REAL)0;
+    r.ca = v.ca[i];
+    r.valid = true;
 }
 
 template <typename REAL, bool ONE>
 __device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, double total_s,
-                                            REAL rh, REAL rw, REAL rl, StageOut<REAL>& o)
+                                            REAL rh, REAL rw, REAL rl, TableRow<REAL>& row,
+                                            StageOut<REAL>& o)
 {
     REAL total_storage = (REAL)total_s;
     REAL river_max_storage = rl * rw * rh;
@@ -537,7 +593,9 @@ __device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, d
         return;
     }
     const int nl = v.K;
-    REAL ca = v.ca[i];
+    const bool in_regs = nl == kRowRegs;
+    if (in_regs && !row.valid) load_row(v, i, row);
+    REAL ca = in_regs ? row.ca : v.ca[i];
     REAL catchment_width = ca / rl;
     REAL width_increment = catchment_width / (REAL)nl;
     int level = 0;
@@ -547,31 +605,34 @@ __device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, d
     REAL prev_total_storage = river_max_storage;
     REAL prev_flood_depth = (REAL)0;
     REAL next_flood_depth = (REAL)0;
-    // The whole table row is loaded up front (independent loads, one memory
-    // latency) and scanned from registers; the scan stops at the first level
-    // the storage does not exceed, exactly as the reference's `break`.
-    REAL H[kMaxFloodLevels];
-    load_row(v.tbl + i * (long)nl, nl, H);
-    bool scanning = true;
-#pragma unroll
-    for (int l = 0; l < kMaxFloodLevels; ++l) {
-        if (l < nl && scanning) {
-            REAL H_curr = H[l];
-            REAL W_curr = rw + (REAL)(l + 1) * width_increment;
-            REAL dS = rl * (REAL)0.5 * (prev_W + W_curr) * (H_curr - prev_H);
-            REAL S_curr = S_accum + dS;
-            next_flood_depth = H_curr;
-            if (total_storage > S_curr) {
-                level += 1;
-                prev_total_storage = S_curr;
-                prev_flood_depth = H_curr;
-                S_accum = S_curr;
-                prev_H = H_curr;
-                prev_W = W_curr;
-            } else {
-                scanning = false;
-            }
+    // The scan stops at the first level the storage does not exceed, exactly
+    // as the reference's `break`.
+    auto level_step = [&](int l, REAL H_curr) -> bool {
+        REAL W_curr = rw + (REAL)(l + 1) * width_increment;
+        REAL dS = rl * (REAL)0.5 * (prev_W + W_curr) * (H_curr - prev_H);
+        REAL S_curr = S_accum + dS;
+        next_flood_depth = H_curr;
+        if (total_storage > S_curr) {
+            level += 1;
+            prev_total_storage = S_curr;
+            prev_flood_depth = H_curr;
+            S_accum = S_curr;
+            prev_H = H_curr;
+            prev_W = W_curr;
+            return true;
         }
+        return false;
+    };
+    if (in_regs) {
+        // row loaded up front (independent loads, one memory latency)
+        bool scanning = true;
+#pragma unroll
+        for (int l = 0; l < kRowRegs; ++l)
+            if (scanning) scanning = level_step(l, row.H[l]);
+    } else {
+        const REAL* trow = v.tbl + i * (long)nl;
+        for (int l = 0; l < nl; ++l)
+            if (!level_step(l, __ldg(trow + l))) break;
     }
     REAL prev_total_width = rw + (REAL)level * width_increment;
     REAL diff_width = (REAL)0;
@@ -610,15 +671,12 @@ template <typename REAL>
 __device__ __forceinline__ REAL clamp01(REAL x) { return fmin(fmax(x, (REAL)0), (REAL)1); }
 
 template <typename REAL, bool ONE>
-__device__ __forceinline__ void levee_stage(const Dev<REAL>& v, long ci, int slot, REAL rh,
+__device__ __forceinline__ void levee_stage(const Dev<REAL>& v, long ci, REAL l_crown,
+                                            REAL l_frac, REAL l_base_h, REAL ca, REAL rh,
                                             REAL rw, REAL rl, StageOut<REAL>& s, double& p_out,
                                             REAL& pdep_out)
 {
     const int nl = v.K;
-    REAL ca = v.ca[ci];
-    REAL l_crown = v.lcrown[slot];
-    REAL l_frac = v.lfrac[slot];
-    REAL l_base_h = v.lbase[slot];
     double riv_sto_curr_hp = s.rs;
     double fld_sto_curr_hp = s.fs;
     double total_sto_hp = riv_sto_curr_hp + fld_sto_curr_hp;
@@ -793,28 +851,17 @@ __device__ __forceinline__ void block_budget(double (&val)[kBudgetTerms], double
 // ---------------------------------------------------------------------------
 // k_stage: cell part
 // ---------------------------------------------------------------------------
-// Per-CTA queue of levee cells awaiting their re-partition (shared memory).
-// Levee cells are a minority scattered through every warp; queueing them and
-// processing the queue densely after a barrier keeps the heavy levee scan off
-// the other lanes and reuses the flood-stage result without a global pass.
-template <typename REAL>
-struct LeveeQueue {
-    int count;
-    int cell[kMaxBlock];
-    int member[kMaxBlock];
-    double rs[kMaxBlock], fs[kMaxBlock];
-    REAL rdep[kMaxBlock], fdep[kMaxBlock], ffr[kMaxBlock];
-    REAL rh[kMaxBlock], rw[kMaxBlock], rl[kMaxBlock];
-};
-
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
 __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, int kh,
-                                           int force_diag, double (&bud)[kBudgetTerms],
-                                           LeveeQueue<REAL>* lq)
+                                           int force_diag, double (&bud)[kBudgetTerms])
 {
-    bool diag;
-    if (!member_step(v.ctl, v.nsub, kh, m, force_diag, diag)) return;
-    const int k = step_index(v.ctl, kh);
+    // Every load of this cell is issued before anything waits on another
+    // load's value: the activity test of a single member is static (the
+    // interval loop only runs k < n), and the upstream gather is unrolled into
+    // independent predicated loads.
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
+    if (!st.active) return;
+    const int k = st.k;
     const double* __restrict__ rsrc = (k & 1) ? v.rs1 : v.rs0;
     const double* __restrict__ fsrc = (k & 1) ? v.fs1 : v.fs0;
     double* __restrict__ rdst = (k & 1) ? v.rs0 : v.rs1;
@@ -829,24 +876,46 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     const double rsto = rsrc[im];
     const double fsto = fsrc[im];
-    const double prot = lev_cell ? v.ps[im] : 0.0;
     const REAL qr = v.qur[im], qf = v.quf[im];
-
+    const REAL ro = par<ONE>(v.runoff, CMF_BATCH_RUNOFF, v.batched, i, m, M);
+    const REAL rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, i, m, M);
+    const REAL rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, i, m, M);
+    const REAL rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, i, m, M);
     // limit rates of this sub-step were computed once per cell by k_limit
     const REAL lr_i = v.lrs[im];
-
-    // upstream inflow: gather the limited fluxes of the upstream cells
-    double rin = 0.0, fin = 0.0, rti = 0.0;
     const int c0 = v.up[i], c1 = upstream_end(v, i);
-    for (int c = c0; c < c1; ++c) {
-        const long cm = ix<ONE>(c, m, M);
-        const REAL cr = v.qur[cm], cf = v.quf[cm];
-        const REAL lr_c = v.lrs[cm];
-        const REAL ur = (cr >= (REAL)0.0) ? cr * lr_c : cr * lr_i;
-        const REAL uf = (cf >= (REAL)0.0) ? cf * lr_c : cf * lr_i;
-        rin += (double)ur;
-        fin += (double)uf;
-        if (res_cell) rti += (double)(ur + uf);
+    const double prot = lev_cell ? v.ps[im] : 0.0;
+
+    // A cell flooded in the previous sub-step will almost surely need its
+    // floodplain row: start those loads now, alongside the upstream gather.
+    TableRow<REAL> row;
+    row.valid = false;
+    if (v.K == kRowRegs && fsto > 0.0) load_row(v, i, row);
+
+    // upstream inflow: gather the limited fluxes of the upstream cells, in
+    // range order, kChildUnroll independent loads at a time
+    double rin = 0.0, fin = 0.0, rti = 0.0;
+    for (int cb = c0; cb < c1; cb += kChildUnroll) {
+        REAL cr[kChildUnroll], cf[kChildUnroll], cl[kChildUnroll];
+#pragma unroll
+        for (int j = 0; j < kChildUnroll; ++j) {
+            if (cb + j < c1) {
+                const long cm = ix<ONE>(cb + j, m, M);
+                cr[j] = v.qur[cm];
+                cf[j] = v.quf[cm];
+                cl[j] = v.lrs[cm];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kChildUnroll; ++j) {
+            if (cb + j < c1) {
+                const REAL ur = (cr[j] >= (REAL)0.0) ? cr[j] * cl[j] : cr[j] * lr_i;
+                const REAL uf = (cf[j] >= (REAL)0.0) ? cf[j] * cl[j] : cf[j] * lr_i;
+                rin += (double)ur;
+                fin += (double)uf;
+                if (res_cell) rti += (double)(ur + uf);
+            }
+        }
     }
 
     // own limited flux (the downstream rate is needed only for negative flux)
@@ -877,7 +946,6 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     const REAL rinf = (REAL)rin;
     const REAL finf = (REAL)fin;
     const REAL gbif = BIF ? (REAL)gb : (REAL)0;
-    const REAL ro = par<ONE>(v.runoff, CMF_BATCH_RUNOFF, v.batched, i, m, M);
     REAL river_delta = (rinf - rout) * ts;
     double river_su = rsto + (double)river_delta;
     REAL flood_delta = (finf - fout - gbif) * ts;
@@ -892,14 +960,10 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     double total_next = river_su + flood_su + prot + (double)external_delta;
     double total_s = total_next > 0.0 ? total_next : 0.0;
 
-    const REAL rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, i, m, M);
-    const REAL rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, i, m, M);
-    const REAL rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, i, m, M);
     StageOut<REAL> s;
-    flood_stage<REAL, ONE>(v, i, m, total_s, rh, rw, rl, s);
-    // Levee cells are re-partitioned afterwards by k_levee (compact over the
-    // levee list); the partition conserves r + f + p, so the budget's end
-    // storage can be taken here.
+    flood_stage<REAL, ONE>(v, i, m, total_s, rh, rw, rl, row, s);
+    // Levee cells are re-partitioned afterwards by k_levee; the partition
+    // conserves r + f + p, so the budget's end storage is taken here.
     const double p_new = 0.0;
 
     if (BUDGET) {
@@ -910,33 +974,19 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
         bud[CMF_BUDGET_CLIP_GAIN] += total_s - raw_next;
         if (mouth) bud[CMF_BUDGET_MOUTH_OUT] += ((double)rout + (double)fout) * (double)ts;
         if (k == 0 || kh == -2) bud[CMF_BUDGET_STORAGE_START] += pre;
-        if (diag) bud[CMF_BUDGET_STORAGE_END] += s.rs + s.fs + p_new;
+        if (st.diag) bud[CMF_BUDGET_STORAGE_END] += s.rs + s.fs + p_new;
     }
 
     v.rout[im] = rout;
     v.fout[im] = fout;
-    if (LEV && lev_cell) {
-        const int q = atomicAdd(&lq->count, 1);
-        lq->cell[q] = (int)i;
-        lq->member[q] = m;
-        lq->rs[q] = s.rs;
-        lq->fs[q] = s.fs;
-        lq->rdep[q] = s.rdep;
-        lq->fdep[q] = s.fdep;
-        lq->ffr[q] = s.ffr;
-        lq->rh[q] = rh;
-        lq->rw[q] = rw;
-        lq->rl[q] = rl;
-    } else {
-        rdst[im] = s.rs;
-        fdst[im] = s.fs;
-        v.rdep[im] = s.rdep;
-        v.fdep[im] = s.fdep;
-        v.ffr[im] = s.ffr;
-        if (diag) v.pdep[im] = s.fdep;
-    }
+    rdst[im] = s.rs;
+    fdst[im] = s.fs;
+    v.rdep[im] = s.rdep;
+    v.fdep[im] = s.fdep;
+    v.ffr[im] = s.ffr;
+    if (!lev_cell && st.diag) v.pdep[im] = s.fdep;
     if (res_cell) v.rti[im] = rti;
-    if (diag) {
+    if (st.diag) {
         if (v.rinf) v.rinf[im] = rin;
         if (v.finf) v.finf[im] = fin;
         if (v.lr) v.lr[im] = lr_i;
@@ -975,9 +1025,9 @@ __global__ void __launch_bounds__(256) k_limit(const Dev<REAL> v, int kh)
     if (t >= v.N * (long)v.M) return;
     long i = ONE ? t : t / v.M;
     int m = ONE ? 0 : (int)(t - i * v.M);
-    bool diag;
-    if (!member_step(v.ctl, v.nsub, kh, m, 2, diag)) return;
-    const int k = step_index(v.ctl, kh);
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
+    if (!st.active) return;
+    const int k = st.k;
     const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
     const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
     v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
@@ -1002,8 +1052,56 @@ __device__ __forceinline__ void advance_step(int* ctl, cudaGraphConditionalHandl
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_levee: levee re-partition (levee.cu:29-261) over the compact levee list,
+// after k_stage wrote the sub-step's flood-stage result.  A kernel of its own:
+// levee cells are a scattered minority, and running their long scan inside
+// k_stage would stretch every CTA of the much larger catchment grid.
+// ---------------------------------------------------------------------------
+template <typename REAL, bool ONE>
+__global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int force_diag,
+                                               cudaGraphConditionalHandle h, int advance)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < v.NLV * (long)v.M) {
+        const long li = ONE ? t : t / v.M;
+        const int m = ONE ? 0 : (int)(t - li * v.M);
+        const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
+        if (st.active) {
+            const int k = st.k;
+            double* rdst = (k & 1) ? v.rs0 : v.rs1;
+            double* fdst = (k & 1) ? v.fs0 : v.fs1;
+            const long ci = v.lci[li];
+            const long cm = ix<ONE>(ci, m, v.M);
+            const REAL l_crown = v.lcrown[li], l_frac = v.lfrac[li], l_base = v.lbase[li];
+            const REAL rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, ci, m, v.M);
+            const REAL rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
+            const REAL rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
+            const REAL ca = v.ca[ci];
+            StageOut<REAL> s;
+            s.rs = rdst[cm];
+            s.fs = fdst[cm];
+            s.rdep = v.rdep[cm];
+            s.fdep = v.fdep[cm];
+            s.ffr = v.ffr[cm];
+            double p_new;
+            REAL pdep_new;
+            levee_stage<REAL, ONE>(v, ci, l_crown, l_frac, l_base, ca, rh, rw, rl, s, p_new,
+                                   pdep_new);
+            rdst[cm] = s.rs;
+            fdst[cm] = s.fs;
+            v.ps[cm] = p_new;
+            v.rdep[cm] = s.rdep;
+            v.fdep[cm] = s.fdep;
+            v.pdep[cm] = pdep_new;
+            v.ffr[cm] = s.ffr;
+        }
+    }
+    if (kh == -1 && advance) advance_step(v.ctl, h, 1);
+}
+
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
-__global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int force_diag,
+__global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int set_cond)
 {
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
@@ -1014,12 +1112,6 @@ __global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int fo
             stage_path<REAL, ONE, BIF>(v, p, m, kh);
         }
     } else {
-        __shared__ LeveeQueue<REAL> lq_storage;
-        LeveeQueue<REAL>* lq = LEV ? &lq_storage : nullptr;
-        if (LEV) {
-            if (threadIdx.x == 0) lq->count = 0;
-            __syncthreads();
-        }
         double bud[kBudgetTerms];
 #pragma unroll
         for (int q = 0; q < kBudgetTerms; ++q) bud[q] = 0.0;
@@ -1027,39 +1119,12 @@ __global__ void __launch_bounds__(256) k_stage(const Dev<REAL> v, int kh, int fo
         if (t < v.N * (long)v.M) {
             long i = ONE ? t : t / v.M;
             int m = ONE ? 0 : (int)(t - i * v.M);
-            stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud, lq);
+            stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud);
         }
         if (BUDGET) block_budget(bud, v.bpart, v.cell_blocks);
-        if (LEV) {
-            __syncthreads();
-            const int k = step_index(v.ctl, kh);
-            double* rdst = (k & 1) ? v.rs0 : v.rs1;
-            double* fdst = (k & 1) ? v.fs0 : v.fs1;
-            for (int q = threadIdx.x; q < lq->count; q += blockDim.x) {
-                const long ci = lq->cell[q];
-                const int m = lq->member[q];
-                const long cm = ix<ONE>(ci, m, v.M);
-                StageOut<REAL> st;
-                st.rs = lq->rs[q];
-                st.fs = lq->fs[q];
-                st.rdep = lq->rdep[q];
-                st.fdep = lq->fdep[q];
-                st.ffr = lq->ffr[q];
-                double p_new;
-                REAL pdep_new;
-                levee_stage<REAL, ONE>(v, ci, v.lslot[ci], lq->rh[q], lq->rw[q], lq->rl[q], st,
-                                       p_new, pdep_new);
-                rdst[cm] = st.rs;
-                fdst[cm] = st.fs;
-                v.ps[cm] = p_new;
-                v.rdep[cm] = st.rdep;
-                v.fdep[cm] = st.fdep;
-                v.pdep[cm] = pdep_new;
-                v.ffr[cm] = st.ffr;
-            }
-        }
     }
-    if (kh == -1) advance_step(v.ctl, h, set_cond);
+    // With levees, k_levee is the last kernel of the sub-step and advances.
+    if (!LEV && kh == -1) advance_step(v.ctl, h, set_cond);
 }
 
 // ---------------------------------------------------------------------------

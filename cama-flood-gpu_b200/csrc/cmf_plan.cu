@@ -37,6 +37,7 @@ struct KernelSet {
     const void* end;
     const void* copy_back;
     const void* limit;
+    const void* levee;
 };
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUD>
@@ -51,6 +52,7 @@ KernelSet make_set()
     k.end = (const void*)k_interval_end<REAL, ONE>;
     k.copy_back = (const void*)k_copy_back<REAL, ONE>;
     k.limit = (const void*)k_limit<REAL, ONE, BIF>;
+    k.levee = (const void*)k_levee<REAL, ONE>;
     return k;
 }
 
@@ -130,6 +132,7 @@ struct CmfPlan {
     int tpb;
     int cell_blocks;
     int path_blocks;
+    int levee_blocks;
     // graph
     bool graph_ready;
     cudaGraph_t graph;
@@ -364,6 +367,13 @@ int build_graph(CmfPlan* p, double T, int fixed_n)
         int set = 1;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
         if ((rc = add_kernel(&b2, body, &bl, 1, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
+        if (p->levee_blocks > 0) {
+            cudaGraphNode_t b3;
+            int adv = 1;
+            void* a3[] = {p->dev, &kh, &fd, &h, &adv};
+            if ((rc = add_kernel(&b3, body, &b2, 1, p->ks.levee, p->levee_blocks, p->tpb, a3)) != CMF_OK)
+                goto fail;
+        }
     }
     {
         const int eb = ceil_div((long)v.num_catchments * v.num_members, 256);
@@ -445,6 +455,9 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
         int set = 0;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
         if ((rc = launch(p->ks.stage, grid, p->tpb, a2, s)) != CMF_OK) return rc;
+        if (p->levee_blocks > 0) {
+            if ((rc = launch(p->ks.levee, p->levee_blocks, p->tpb, a2, s)) != CMF_OK) return rc;
+        }
     }
     {
         void* args[] = {p->dev};
@@ -551,6 +564,9 @@ int cmf_plan_create(const CmfView* view, CmfPlan** out)
     p->path_blocks = (f & CMF_FEAT_BIFURCATION)
                          ? ceil_div((long)view->num_bifurcation_paths * view->num_members, p->tpb)
                          : 0;
+    p->levee_blocks = (f & CMF_FEAT_LEVEE)
+                          ? ceil_div((long)view->num_levees * view->num_members, p->tpb)
+                          : 0;
     const bool res = f & CMF_FEAT_RESERVOIR, lev = f & CMF_FEAT_LEVEE,
                bif = f & CMF_FEAT_BIFURCATION, bud = f & CMF_FEAT_BUDGET;
     Layout L = layout_of(view, p->cell_blocks);
@@ -650,6 +666,10 @@ int cmf_phase_stage(CmfPlan* p, void* stream, int diag)
     void* args[] = {p->dev, &kh, &fd, &h, &set};
     rc = launch(p->ks.stage, p->cell_blocks + p->path_blocks, p->tpb, args, s);
     if (rc != CMF_OK) return rc;
+    if (p->levee_blocks > 0) {
+        rc = launch(p->ks.levee, p->levee_blocks, p->tpb, args, s);
+        if (rc != CMF_OK) return rc;
+    }
     void* a2[] = {p->dev};
     return launch(p->ks.copy_back,
                   ceil_div((long)p->view.num_catchments * p->view.num_members, 256), 256, a2, s);
@@ -714,6 +734,13 @@ int cmf_launch_substep(CmfPlan* p, void* stream, int32_t k, int part)
         int set = 0;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
         return launch(p->ks.stage, grid, p->tpb, a2, s);
+    }
+    if (part == CMF_PART_LEVEE) {
+        if (p->levee_blocks == 0) return CMF_OK;
+        cudaGraphConditionalHandle h = 0;
+        int set = 0;
+        void* a3[] = {p->dev, &kh, &fd, &h, &set};
+        return launch(p->ks.levee, p->levee_blocks, p->tpb, a3, s);
     }
     if (part == CMF_PART_END) {
         void* args[] = {p->dev};
@@ -810,6 +837,7 @@ extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
     p.tpb = block_of(&v);
     p.cell_blocks = ceil_div((long)v.num_catchments, p.tpb);
     p.path_blocks = (f & CMF_FEAT_BIFURCATION) ? ceil_div((long)v.num_bifurcation_paths, p.tpb) : 0;
+    p.levee_blocks = (f & CMF_FEAT_LEVEE) ? ceil_div((long)v.num_levees, p.tpb) : 0;
     const bool res = f & CMF_FEAT_RESERVOIR, lev = f & CMF_FEAT_LEVEE,
                bif = f & CMF_FEAT_BIFURCATION, bud = f & CMF_FEAT_BUDGET;
     Layout L = layout_of(&v, p.cell_blocks);

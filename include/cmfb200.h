@@ -256,13 +256,15 @@ int cmf_phase_fixed_dt(CmfPlan* plan, void* stream, double outer_seconds,
 /* One kernel of sub-step k of the current interval (after cmf_phase_cfl or
  * cmf_phase_fixed_dt), launched directly on `stream` so a caller can time it
  * with events: part = CMF_PART_MOMENTUM, CMF_PART_LIMIT (the per-cell limit
- * rate), CMF_PART_STAGE, or CMF_PART_END (the interval epilogue, after the
- * last sub-step).  Running MOMENTUM, LIMIT and STAGE for k = 0..n-1 then END
- * is exactly cmf_step_interval without the graph. */
+ * rate), CMF_PART_STAGE, CMF_PART_LEVEE (the levee re-partition, a no-op
+ * without levees) or CMF_PART_END (the interval epilogue, after the last
+ * sub-step).  Running MOMENTUM, LIMIT, STAGE and LEVEE for k = 0..n-1 then
+ * END is exactly cmf_step_interval without the graph. */
 #define CMF_PART_MOMENTUM 1
 #define CMF_PART_STAGE 2
 #define CMF_PART_END 4
 #define CMF_PART_LIMIT 8
+#define CMF_PART_LEVEE 16
 int cmf_launch_substep(CmfPlan* plan, void* stream, int32_t k, int part);
 /* One sub-step (momentum, limit rate, stage) of a single-member view that
  * allocates nothing.  No counterpart in the reference.  It is for callers that
