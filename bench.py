@@ -168,6 +168,79 @@ def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15
     }
 
 
+def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -> dict:
+    """The batched-ensemble workload at reduced size: `members` members of a
+    `basins`-basin network (~`catchments` catchments per member, runoff and
+    river Manning perturbed per member, daily forcing, per-member dt).  One
+    simulated day in a single member-innermost model (one launch per phase)
+    against the same members run one after another as plain models, both from
+    the same initial state on the same GPU."""
+    import torch
+    from cmfb200 import CaMaFlood, synthetic as syn
+    net = syn.generate_basins(basins, catchments, seed=3)
+    n = net.num_catchments
+    rfac, mfac = syn.ensemble_factors(n, members, seed=3)
+    manning = (net.fields["river_manning"][:, None] * mfac).astype(np.float32)
+    mods = ["base", "adaptive_time"]
+    ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=mods,
+                    num_members=members, batched_fields={"river_manning": manning})
+    order = ens.order
+    rm = (syn.daily_runoff(net, 0)[:, None] * rfac).astype(np.float32)[order]
+    forcing = torch.as_tensor(rm).to(device)
+    init = {k: v.clone() for k, v in ens.state_tensors().items()}
+    stream = torch.cuda.current_stream(device)
+
+    def reset(model, state):
+        for k, v in model.state_tensors().items():
+            v.copy_(state[k])
+
+    ens.set_inputs(forcing)
+    ens.step_advance()                      # builds the interval graph
+    reset(ens, init)
+    torch.cuda.synchronize(device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ens.set_inputs(forcing)
+    ens.step_advance()
+    b.record(stream)
+    torch.cuda.synchronize(device)
+    t_batched = a.elapsed_time(b) / 1e3
+    n_batched = int(ens.sub_step_counts().sum().item())
+    ens.close()
+    del ens, init
+
+    plain = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=mods)
+    init = {k: v.clone() for k, v in plain.state_tensors().items()}
+    man_dev = torch.as_tensor(np.ascontiguousarray(manning[order].T)).to(device)
+    run_dev = torch.as_tensor(np.ascontiguousarray(rm.T)).to(device)
+    plain.base.river_manning.copy_(man_dev[0])
+    plain.set_inputs(run_dev[0])
+    plain.step_advance()                    # graph build
+    torch.cuda.synchronize(device)
+    n_looped = 0
+    a.record(stream)
+    counts = torch.zeros(members, dtype=torch.int32, device=device)
+    for m in range(members):
+        reset(plain, init)
+        plain.base.river_manning.copy_(man_dev[m])
+        plain.set_inputs(run_dev[m])
+        plain.step_advance()
+        counts[m].copy_(plain.sub_step_counts()[0])
+    b.record(stream)
+    torch.cuda.synchronize(device)
+    t_looped = a.elapsed_time(b) / 1e3
+    n_looped = int(counts.sum().item())
+    plain.close()
+    batched = n * n_batched / t_batched
+    looped = n * n_looped / t_looped
+    return {"value": batched, "looped_value": looped, "speedup": batched / looped,
+            "unit": UNIT, "members": members, "catchments_per_member": n, "basins": basins,
+            "sub_steps_per_member_mean": n_batched / members,
+            "workload": "1 day of a member-innermost ensemble (runoff x lognormal(0.3), "
+                        "river Manning x U(0.8,1.2) per member) vs the members looped as "
+                        "plain models; includes the state reset copies of the looped runs"}
+
+
 def run_reference(args) -> None:
     """CPU restatement of the reference path on all host cores (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -359,6 +432,11 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(net, cfg, None)
 
+    ensemble = None
+    if world == 1 and args.ensemble_members > 0:
+        model.close()
+        ensemble = ensemble_compare(device, args.ensemble_members, args.ensemble_catchments)
+
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -381,6 +459,7 @@ def run_ours(args) -> None:
                          "ms_momentum": t_mom, "ms_limit": t_lim, "ms_stage": t_stage,
                          "ms_levee": t_lev},
             "cpu_baseline": cpu,
+            "ensemble": ensemble,
             "clocks": clocks,
             "gpu_launches": launches,
         }
@@ -399,6 +478,10 @@ def main() -> None:
     ap.add_argument("--workload", default="full_6m")
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble-members", type=int, default=64,
+                    help="members of the batched-vs-looped comparison (0 skips it)")
+    ap.add_argument("--ensemble-catchments", type=int, default=600_000,
+                    help="catchments per member of that comparison (the full workload has ~6M)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

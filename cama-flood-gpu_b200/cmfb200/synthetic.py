@@ -232,3 +232,40 @@ CONFIGS = {
                                      levee_fraction=0.2, reservoirs=7_000),
                     days=10, interval=3600.0, max_sub_step_seconds=0.0),
 }
+
+
+def generate_basins(num_basins: int, total_catchments: int, seed: int = 0,
+                    min_size: int = 100, max_size: int = 200_000) -> Network:
+    """Independent single-mouth basins of log-uniform size, concatenated.
+
+    Sizes are drawn log-uniform in [min_size, max_size] and then scaled so that
+    they sum to about `total_catchments` (the ensemble workload: 500 basins,
+    ~6M catchments per member).  Each basin is one tree from `generate` with
+    its last cell as the only mouth; ids and `catchment_basin_id` are offset
+    per basin."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(min_size), np.log(max_size), size=num_basins))
+    sizes = np.maximum(np.round(sizes * total_catchments / sizes.sum()), 2).astype(np.int64)
+    parts = []
+    offset = 0
+    for b, size in enumerate(sizes):
+        net = generate(NetworkSpec(int(size), seed=seed * 100_003 + b + 1, mouth_fraction=0.0))
+        f = dict(net.fields)
+        f["catchment_id"] = f["catchment_id"] + offset
+        f["downstream_id"] = f["downstream_id"] + offset
+        f["catchment_basin_id"] = np.full(int(size), b, dtype=np.int64)
+        parts.append(f)
+        offset += int(size)
+    fields = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+    spec = NetworkSpec(int(offset), seed=seed, mouth_fraction=0.0)
+    return Network(spec=spec, fields=fields, info={"basin_sizes": sizes})
+
+
+def ensemble_factors(num_catchments: int, members: int, seed: int = 0):
+    """Per-member perturbations of the ensemble workload, member-innermost:
+    a multiplicative lognormal(sigma 0.3) runoff factor per catchment and a
+    uniform +-20 % river-Manning factor, both [N, M] float32."""
+    rng = np.random.default_rng([seed, 31337])
+    runoff = np.exp(0.3 * rng.standard_normal((num_catchments, members))).astype(np.float32)
+    manning = rng.uniform(0.8, 1.2, size=(num_catchments, members)).astype(np.float32)
+    return runoff, manning

@@ -1163,6 +1163,16 @@ __global__ void __launch_bounds__(256) k_cfl(const Dev<REAL> v)
             for (int o = 16; o > 0; o >>= 1) x = max(x, __shfl_down_sync(0xffffffffu, x, o));
             if (lane == 0 && x > 0) atomicMax(&v.nsub[0], x);
         }
+    } else if (v.M <= (int)blockDim.x) {
+        // per-member maximum inside the block (shared-memory atomics), then
+        // one global atomic per member and block
+        __shared__ int smax[kMaxBlock];
+        if ((int)threadIdx.x < v.M) smax[threadIdx.x] = 0;
+        __syncthreads();
+        if (t < v.N * (long)v.M) atomicMax(&smax[m], n_steps);
+        __syncthreads();
+        if ((int)threadIdx.x < v.M && smax[threadIdx.x] > 0)
+            atomicMax(&v.nsub[threadIdx.x], smax[threadIdx.x]);
     } else {
         if (t < v.N * (long)v.M) atomicMax(&v.nsub[m], n_steps);
     }
