@@ -231,6 +231,11 @@ CONFIGS = {
     "full_6m": dict(spec=NetworkSpec(6_000_000, seed=2, bifurcation_paths=200_000,
                                      levee_fraction=0.2, reservoirs=7_000),
                     days=10, interval=3600.0, max_sub_step_seconds=0.0),
+    # the same physics at a third of the size: one sub-step touches ~410 MB,
+    # above the 126 MB L2, while a multi-pass profiler capture stays small
+    "full_2m": dict(spec=NetworkSpec(2_000_000, seed=2, bifurcation_paths=66_667,
+                                     levee_fraction=0.2, reservoirs=2_333),
+                    days=10, interval=3600.0, max_sub_step_seconds=0.0),
 }
 
 
