@@ -241,6 +241,80 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
                         "plain models; includes the state reset copies of the looped runs"}
 
 
+def adjoint_compare(device, days: int, checkpoint_every: int = 96,
+                    catchments: int = 250_000) -> dict:
+    """Forward+adjoint against forward on the calibration window: the
+    250k-catchment network of the full-physics config with the base physics
+    only (the adjoint covers no bifurcation, levee or reservoir), fp64, daily
+    forcing over `days` intervals, discharge at 500 cells with upstream area
+    > 1000 km^2, relative-misfit loss against a run with river Manning x
+    lognormal(0.2).  Both are timed with CUDA events on the same GPU from the
+    same spun-up state; the gradient run includes its checkpointed forward."""
+    import torch
+    from cmfb200 import CaMaFlood, synthetic as syn, topology
+    from cmfb200.adjoint import AdjointRouting
+    net = syn.generate(syn.NetworkSpec(catchments, seed=1, levee_fraction=0.0))
+    model = CaMaFlood(device=device, input_proxy=net.fields,
+                      opened_modules=["base", "adaptive_time"], precision="float64")
+    model.set_inputs(torch.as_tensor(syn.daily_runoff(net, 0)[model.order]).to(device))
+    model.step_advance()
+    fx = model.export_fields()
+    area = topology.accumulate_upstream(fx["downstream_idx"], fx["catchment_area"].astype(np.float64))
+    rng = np.random.default_rng(4)
+    cand = np.flatnonzero(area > 1.0e9)
+    gauges = np.sort(rng.choice(cand, size=min(500, cand.size), replace=False))
+    eng = AdjointRouting(model, gauges, checkpoint_every=checkpoint_every)
+    forcing = torch.as_tensor(np.stack([syn.daily_runoff(net, 1 + d)[model.order]
+                                        for d in range(days)]), dtype=torch.float64, device=device)
+    params = eng.parameters()
+    state0 = eng.initial_state()
+    truth = dict(params)
+    truth["river_manning"] = params["river_manning"] * torch.as_tensor(
+        np.exp(0.2 * rng.standard_normal(eng.N)), device=device)
+    q_obs, _ = eng.forward_only(truth, forcing, state0)
+    stream = torch.cuda.current_stream(device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def fwd():
+        return eng.forward_only(params, forcing, state0)
+
+    def fwd_adj():
+        p = {k: v.clone().requires_grad_(True) for k, v in params.items()}
+        f = forcing.clone().requires_grad_(True)
+        q, _ = eng.window(p, f, state0)
+        loss = (((q - q_obs) / q_obs) ** 2).sum()
+        return torch.autograd.grad(loss, [p["river_manning"], p["river_height"],
+                                          p["river_width"], f])
+
+    fwd()
+    fwd_adj()                                 # warm-up (allocations, lazy init)
+    torch.cuda.synchronize(device)
+    ev[0].record(stream)
+    fwd()
+    ev[1].record(stream)
+    torch.cuda.synchronize(device)
+    ev[2].record(stream)
+    fwd_adj()
+    ev[3].record(stream)
+    torch.cuda.synchronize(device)
+    t_fwd = ev[0].elapsed_time(ev[1]) / 1e3
+    t_adj = ev[2].elapsed_time(ev[3]) / 1e3
+    # sub-step count of the window (the CFL counts of the primal run)
+    _, _, counts, _, _ = eng._forward(params["river_manning"], params["flood_manning"],
+                                      params["river_height"], params["river_width"], forcing,
+                                      state0, keep_checkpoints=False)
+    subs = int(sum(counts))
+    model.close()
+    n = eng.N
+    return {"fwd_value": n * subs / t_fwd, "fwd_adj_value": n * subs / t_adj, "unit": UNIT,
+            "fwd_adj_over_fwd": t_adj / t_fwd, "catchments": n, "sub_steps": subs,
+            "days": days, "checkpoint_every": checkpoint_every, "gauges": int(gauges.size),
+            "dtype": "f64",
+            "workload": "base-physics 250k network, fp64, daily forcing, gradients w.r.t. "
+                        "river Manning, river height, river width and runoff; fwd = the same "
+                        "primal kernels without checkpoints"}
+
+
 def run_reference(args) -> None:
     """CPU restatement of the reference path on all host cores (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -437,6 +511,11 @@ def run_ours(args) -> None:
         model.close()
         ensemble = ensemble_compare(device, args.ensemble_members, args.ensemble_catchments)
 
+    adjoint = None
+    if world == 1 and args.adjoint_days > 0:
+        model.close()
+        adjoint = adjoint_compare(device, args.adjoint_days)
+
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -460,6 +539,7 @@ def run_ours(args) -> None:
                          "ms_levee": t_lev},
             "cpu_baseline": cpu,
             "ensemble": ensemble,
+            "adjoint": adjoint,
             "clocks": clocks,
             "gpu_launches": launches,
         }
@@ -480,6 +560,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64,
                     help="members of the batched-vs-looped comparison (0 skips it)")
+    ap.add_argument("--adjoint-days", type=int, default=30,
+                    help="daily intervals of the forward+adjoint comparison (0 = skip)")
     ap.add_argument("--ensemble-catchments", type=int, default=600_000,
                     help="catchments per member of that comparison (the full workload has ~6M)")
     args = ap.parse_args()

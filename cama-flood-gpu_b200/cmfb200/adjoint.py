@@ -1,0 +1,247 @@
+"""Differentiable routing windows over the hand-written CUDA adjoint.
+
+`RoutingWindow` is a `torch.autograd.Function`: its forward runs a window of
+forcing intervals through the fp64 primal kernels of libcmfb200
+(`cmf_adj_forward`), storing the state every `checkpoint_every` sub-steps;
+its backward recomputes each checkpoint segment with a tape and sweeps it in
+reverse (`cmf_adj_reverse`).  The gradients reach the river and floodplain
+Manning coefficients, river height, river width, the runoff of every interval
+and the initial state.
+
+The sub-step counts of the intervals come from the CFL rule on the state at
+each interval start (cmfgpu/phys/cuda/adaptive_time.cu:19-48) and carry no
+gradient, like `floor` and `.item()` in the reference's step
+(cmfgpu/models/cama_flood_model.py:119-132).
+
+State layout: a [9, N] fp64 tensor in model (breadth-first) order, field
+order `STATE`.  Parameters and forcing are model-ordered fp64 tensors.
+"""
+from __future__ import annotations
+
+import bisect
+import ctypes
+
+import torch
+
+from . import _lib
+
+STATE = ("river_storage", "flood_storage", "river_outflow", "flood_outflow", "river_depth",
+         "flood_depth", "river_cross_section_depth", "flood_cross_section_depth",
+         "flood_cross_section_area")
+PARAMS = ("river_manning", "flood_manning", "river_height", "river_width")
+F_ROUT, F_FOUT = 2, 3
+
+
+def _bind(h) -> None:
+    if getattr(h, "_adj_bound", False):
+        return
+    P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    h.cmf_adj_layout.restype = I
+    h.cmf_adj_layout.argtypes = [ctypes.POINTER(I)] * 4
+    h.cmf_adj_plan_create.restype = I
+    h.cmf_adj_plan_create.argtypes = [ctypes.POINTER(_lib.CmfView), ctypes.POINTER(P)]
+    h.cmf_adj_plan_destroy.restype = None
+    h.cmf_adj_plan_destroy.argtypes = [P]
+    h.cmf_adj_sub_steps.restype = I
+    h.cmf_adj_sub_steps.argtypes = [P, P, P, D, P]
+    h.cmf_adj_forward.restype = I
+    h.cmf_adj_forward.argtypes = [P, P, P, I, I, P, D]
+    h.cmf_adj_reverse.restype = I
+    h.cmf_adj_reverse.argtypes = [P, P, P, I, P, D, P, P, P, P]
+    h.cmf_adj_finalize.restype = I
+    h.cmf_adj_finalize.argtypes = [P, P, P, P, P]
+    h._adj_bound = True
+
+
+class AdjointRouting:
+    """Gradient engine bound to a `CaMaFlood` model.
+
+    The model must use precision "float64", one member and the base physics
+    (modules base / adaptive_time); its topology and fixed geometry are used,
+    while the four differentiated parameters are passed per window.
+
+    gauges            model-order indices of the cells whose discharge
+                      (river + floodplain outflow at each interval end) the
+                      window returns
+    checkpoint_every  sub-steps between stored states (the recompute segment)
+    """
+
+    def __init__(self, model, gauges, checkpoint_every: int = 96):
+        if model.precision != "float64":
+            raise ValueError("the adjoint runs in fp64: build the model with precision='float64'")
+        if model.num_members != 1:
+            raise ValueError("the adjoint takes a single-member model")
+        if model.bifurcation is not None or model.levee is not None or model.reservoir is not None:
+            raise NotImplementedError("the adjoint covers the base physics (no bifurcation, "
+                                      "levee or reservoir modules)")
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        self.model = model
+        self.device = model.device
+        self.N = model.num_catchments
+        self.outer = model.step_seconds
+        self.K = int(checkpoint_every)
+        self.gauges = torch.as_tensor(gauges, dtype=torch.long, device=self.device)
+        self.lib = _lib.lib()
+        _bind(self.lib)
+        cnt = [ctypes.c_int() for _ in range(4)]
+        _lib.check(self.lib.cmf_adj_layout(*[ctypes.byref(c) for c in cnt]), "adj_layout")
+        self.n_state, self.n_slot, self.n_scratch, self.n_grad = (c.value for c in cnt)
+        assert self.n_state == len(STATE) and self.n_grad == len(PARAMS)
+        self._n_dev = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    # ------------------------------------------------------------------ #
+    def initial_state(self) -> torch.Tensor:
+        """The model's current state as a [9, N] fp64 tensor."""
+        b = self.model.base
+        return torch.stack([getattr(b, k).detach().to(torch.float64) for k in STATE]).contiguous()
+
+    def parameters(self) -> dict[str, torch.Tensor]:
+        """Copies of the model's four differentiable parameters."""
+        b = self.model.base
+        return {k: getattr(b, k).detach().clone() for k in PARAMS}
+
+    def _plan(self, rman, fman, rh, rw):
+        v = self.model._view()
+        v.river_manning = rman.data_ptr()
+        v.flood_manning = fman.data_ptr()
+        v.river_height = rh.data_ptr()
+        v.river_width = rw.data_ptr()
+        plan = ctypes.c_void_p()
+        _lib.check(self.lib.cmf_adj_plan_create(ctypes.byref(v), ctypes.byref(plan)),
+                   "adj_plan_create")
+        return plan
+
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _sub_steps(self, plan, slot: torch.Tensor) -> int:
+        _lib.check(self.lib.cmf_adj_sub_steps(plan, self._stream(), slot.data_ptr(), self.outer,
+                                              self._n_dev.data_ptr()), "adj_sub_steps")
+        n = int(self._n_dev.item())
+        if n < 1 or n > 100_000:
+            raise FloatingPointError(f"CFL sub-step count {n} out of range (non-finite depth?)")
+        return n
+
+    def window(self, params: dict, forcing: torch.Tensor, state0: torch.Tensor):
+        """Differentiable window: returns (discharge [T, G], final state [9, N])."""
+        return RoutingWindow.apply(self, params["river_manning"], params["flood_manning"],
+                                   params["river_height"], params["river_width"], forcing, state0)
+
+    @torch.no_grad()
+    def forward_only(self, params: dict, forcing: torch.Tensor, state0: torch.Tensor):
+        """The window's forward without checkpoints (for timing and FD checks)."""
+        out = self._forward(params["river_manning"], params["flood_manning"],
+                            params["river_height"], params["river_width"], forcing, state0,
+                            keep_checkpoints=False)
+        return out[0], out[1]
+
+    # ------------------------------------------------------------------ #
+    def _prep(self, *ts):
+        return [t.detach().to(device=self.device, dtype=torch.float64).contiguous() for t in ts]
+
+    def _forward(self, rman, fman, rh, rw, forcing, state0, keep_checkpoints=True):
+        rman, fman, rh, rw, forcing, state0 = self._prep(rman, fman, rh, rw, forcing, state0)
+        N, S = self.N, self.n_slot
+        if state0.shape != (self.n_state, N) or forcing.dim() != 2 or forcing.shape[1] != N:
+            raise ValueError("state0 must be [9, N] and forcing [T, N] in model order")
+        plan = self._plan(rman, fman, rh, rw)
+        try:
+            slots = torch.empty((2, S, N), dtype=torch.float64, device=self.device)
+            slots[0, :self.n_state].copy_(state0)
+            stream = self._stream()
+            T = forcing.shape[0]
+            q = torch.empty((T, self.gauges.numel()), dtype=torch.float64, device=self.device)
+            counts, ckpts, g = [], {}, 0
+            for t in range(T):
+                n = self._sub_steps(plan, slots[0])
+                dt = self.outer / n
+                k = 0
+                while k < n:
+                    if keep_checkpoints and g % self.K == 0:
+                        ckpts[g] = slots[0, :self.n_state].clone()
+                    m = min(n - k, self.K - g % self.K)
+                    _lib.check(self.lib.cmf_adj_forward(plan, stream, slots.data_ptr(), m, 0,
+                                                        forcing[t].data_ptr(), dt), "adj_forward")
+                    if m & 1:
+                        slots[0, :self.n_state].copy_(slots[1, :self.n_state])
+                    k += m
+                    g += m
+                counts.append(n)
+                q[t] = (slots[0, F_ROUT] + slots[0, F_FOUT])[self.gauges]
+            final = slots[0, :self.n_state].clone()
+        finally:
+            self.lib.cmf_adj_plan_destroy(plan)
+        return q, final, counts, ckpts, (rman, fman, rh, rw, forcing)
+
+    def _backward(self, saved, counts, ckpts, q_bar, state_bar):
+        rman, fman, rh, rw, forcing = saved
+        N, S, dev = self.N, self.n_slot, self.device
+        T = forcing.shape[0]
+        dts = [self.outer / n for n in counts]
+        starts, ends, acc = [], [], 0
+        for n in counts:
+            starts.append(acc)
+            acc += n
+            ends.append(acc)
+        total = acc
+        lam = torch.zeros((self.n_state, N), dtype=torch.float64, device=dev)
+        if state_bar is not None:
+            lam += state_bar.to(dev, torch.float64)
+        grad = torch.zeros((self.n_grad, N), dtype=torch.float64, device=dev)
+        g_forcing = torch.zeros((T, N), dtype=torch.float64, device=dev)
+        scratch = torch.zeros((self.n_scratch, N), dtype=torch.float64, device=dev)
+        tape = torch.empty((min(self.K, max(total, 1)) + 1, S, N), dtype=torch.float64, device=dev)
+        stride = S * N * 8
+        plan = self._plan(rman, fman, rh, rw)
+        stream = self._stream()
+        try:
+            n_seg = (total + self.K - 1) // self.K
+            for s in range(n_seg - 1, -1, -1):
+                g0, g1 = s * self.K, min((s + 1) * self.K, total)
+                tape[0, :self.n_state].copy_(ckpts[g0])
+                chunks, g = [], g0
+                while g < g1:
+                    t = bisect.bisect_right(starts, g) - 1
+                    m = min(g1, ends[t]) - g
+                    _lib.check(self.lib.cmf_adj_forward(plan, stream, tape.data_ptr() + (g - g0) * stride,
+                                                        m, 1, forcing[t].data_ptr(), dts[t]),
+                               "adj_forward(tape)")
+                    chunks.append((t, g - g0, m))
+                    g += m
+                for t, j0, m in reversed(chunks):
+                    if q_bar is not None and g0 + j0 + m == ends[t]:
+                        qb = q_bar[t].to(dev, torch.float64)
+                        lam[F_ROUT].index_add_(0, self.gauges, qb)
+                        lam[F_FOUT].index_add_(0, self.gauges, qb)
+                    _lib.check(self.lib.cmf_adj_reverse(
+                        plan, stream, tape.data_ptr() + j0 * stride, m, forcing[t].data_ptr(),
+                        dts[t], lam.data_ptr(), grad.data_ptr(), g_forcing[t].data_ptr(),
+                        scratch.data_ptr()), "adj_reverse")
+            _lib.check(self.lib.cmf_adj_finalize(plan, stream, lam.data_ptr(), grad.data_ptr(),
+                                                 scratch.data_ptr()), "adj_finalize")
+        finally:
+            self.lib.cmf_adj_plan_destroy(plan)
+        return grad, g_forcing, lam
+
+
+class RoutingWindow(torch.autograd.Function):
+    """(engine, river_manning, flood_manning, river_height, river_width,
+    forcing [T, N], state0 [9, N]) -> (discharge at the gauges [T, G],
+    final state [9, N]); all fp64, model order."""
+
+    @staticmethod
+    def forward(ctx, engine, rman, fman, rh, rw, forcing, state0):
+        q, final, counts, ckpts, saved = engine._forward(rman, fman, rh, rw, forcing, state0)
+        ctx.engine = engine
+        ctx.counts = counts
+        ctx.ckpts = ckpts
+        ctx.saved = saved
+        return q, final
+
+    @staticmethod
+    def backward(ctx, q_bar, state_bar):
+        grad, g_forcing, lam = ctx.engine._backward(ctx.saved, ctx.counts, ctx.ckpts, q_bar,
+                                                    state_bar)
+        ctx.ckpts = None
+        return None, grad[0], grad[1], grad[2], grad[3], g_forcing, lam

@@ -78,7 +78,16 @@ def init_river_depth(catchment_elevation, river_height, downstream_idx, visit=No
 
 
 def accumulate_upstream(downstream_idx, values) -> np.ndarray:
+    """Sum of `values` over each cell and everything upstream of it.  Takes a
+    topological order (downstream cells after their upstream cells) or its
+    reverse, such as the model's breadth-first order from the mouths."""
     dn = np.ascontiguousarray(downstream_idx, dtype=np.int32)
+    n = dn.shape[0]
+    idx = np.arange(n)
+    inner = dn != idx
+    if n and inner.any() and (dn[inner] < idx[inner]).all():
+        flipped = accumulate_upstream((n - 1 - dn)[::-1], np.asarray(values)[::-1])
+        return np.ascontiguousarray(flipped[::-1])
     v = np.ascontiguousarray(values, dtype=np.float64)
     out = np.empty_like(v)
     _lib.check(_lib.lib().cmf_topo_accumulate_upstream(dn.shape[0], _ptr(dn), _ptr(v), _ptr(out)),
