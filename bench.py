@@ -299,6 +299,26 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96,
     torch.cuda.synchronize(device)
     t_fwd = ev[0].elapsed_time(ev[1]) / 1e3
     t_adj = ev[2].elapsed_time(ev[3]) / 1e3
+    # the product's own fp64 forward (interval graphs) over the same window
+    snap = {k: v.clone() for k, v in model.state_tensors().items()}
+    b = model.base
+    for k in ("river_manning", "flood_manning", "river_height", "river_width"):
+        getattr(b, k).copy_(params[k])
+
+    def product_fwd():
+        for k, v in model.state_tensors().items():
+            v.copy_(snap[k])
+        for d in range(days):
+            model.set_inputs(forcing[d])
+            model.step_advance()
+
+    product_fwd()
+    torch.cuda.synchronize(device)
+    ev[0].record(stream)
+    product_fwd()
+    ev[1].record(stream)
+    torch.cuda.synchronize(device)
+    t_prod = ev[0].elapsed_time(ev[1]) / 1e3
     # sub-step count of the window (the CFL counts of the primal run)
     _, _, counts, _, _ = eng._forward(params["river_manning"], params["flood_manning"],
                                       params["river_height"], params["river_width"], forcing,
@@ -307,12 +327,15 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96,
     model.close()
     n = eng.N
     return {"fwd_value": n * subs / t_fwd, "fwd_adj_value": n * subs / t_adj, "unit": UNIT,
-            "fwd_adj_over_fwd": t_adj / t_fwd, "catchments": n, "sub_steps": subs,
+            "fwd_adj_over_fwd": t_adj / t_fwd,
+            "product_fwd_value": n * subs / t_prod, "fwd_adj_over_product_fwd": t_adj / t_prod,
+            "catchments": n, "sub_steps": subs,
             "days": days, "checkpoint_every": checkpoint_every, "gauges": int(gauges.size),
             "dtype": "f64",
             "workload": "base-physics 250k network, fp64, daily forcing, gradients w.r.t. "
                         "river Manning, river height, river width and runoff; fwd = the same "
-                        "primal kernels without checkpoints"}
+                        "primal kernels without checkpoints; product_fwd = CaMaFlood.step_advance "
+                        "in fp64 (interval graphs) over the same window"}
 
 
 def run_reference(args) -> None:

@@ -191,35 +191,63 @@ class AdjointRouting:
         grad = torch.zeros((self.n_grad, N), dtype=torch.float64, device=dev)
         g_forcing = torch.zeros((T, N), dtype=torch.float64, device=dev)
         scratch = torch.zeros((self.n_scratch, N), dtype=torch.float64, device=dev)
-        tape = torch.empty((min(self.K, max(total, 1)) + 1, S, N), dtype=torch.float64, device=dev)
+        seg_len = min(self.K, max(total, 1))
+        # Two tapes: segment s-1 is recomputed on a side stream while segment s
+        # is swept in reverse on the caller's stream (the two are independent).
+        tapes = [torch.empty((seg_len + 1, S, N), dtype=torch.float64, device=dev) for _ in range(2)]
         stride = S * N * 8
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(main)
+        for tp in tapes:
+            tp.record_stream(side)
+        ready = [torch.cuda.Event(), torch.cuda.Event()]
+        free = [torch.cuda.Event(), torch.cuda.Event()]
         plan = self._plan(rman, fman, rh, rw)
-        stream = self._stream()
-        try:
-            n_seg = (total + self.K - 1) // self.K
-            for s in range(n_seg - 1, -1, -1):
-                g0, g1 = s * self.K, min((s + 1) * self.K, total)
+
+        def recompute(s: int, buf: int):
+            g0, g1 = s * self.K, min((s + 1) * self.K, total)
+            tape = tapes[buf]
+            chunks, g = [], g0
+            with torch.cuda.stream(side):
                 tape[0, :self.n_state].copy_(ckpts[g0])
-                chunks, g = [], g0
                 while g < g1:
                     t = bisect.bisect_right(starts, g) - 1
                     m = min(g1, ends[t]) - g
-                    _lib.check(self.lib.cmf_adj_forward(plan, stream, tape.data_ptr() + (g - g0) * stride,
-                                                        m, 1, forcing[t].data_ptr(), dts[t]),
-                               "adj_forward(tape)")
+                    _lib.check(self.lib.cmf_adj_forward(
+                        plan, side.cuda_stream, tape.data_ptr() + (g - g0) * stride, m, 1,
+                        forcing[t].data_ptr(), dts[t]), "adj_forward(tape)")
                     chunks.append((t, g - g0, m))
                     g += m
+            ready[buf].record(side)
+            return g0, chunks
+
+        try:
+            n_seg = (total + self.K - 1) // self.K
+            pending = recompute(n_seg - 1, 0) if n_seg else None
+            for idx, s in enumerate(range(n_seg - 1, -1, -1)):
+                buf = idx & 1
+                g0, chunks = pending
+                if s > 0:
+                    if idx >= 1:
+                        side.wait_event(free[1 - buf])
+                    pending = recompute(s - 1, 1 - buf)
+                main.wait_event(ready[buf])
+                tape = tapes[buf]
                 for t, j0, m in reversed(chunks):
                     if q_bar is not None and g0 + j0 + m == ends[t]:
                         qb = q_bar[t].to(dev, torch.float64)
                         lam[F_ROUT].index_add_(0, self.gauges, qb)
                         lam[F_FOUT].index_add_(0, self.gauges, qb)
                     _lib.check(self.lib.cmf_adj_reverse(
-                        plan, stream, tape.data_ptr() + j0 * stride, m, forcing[t].data_ptr(),
-                        dts[t], lam.data_ptr(), grad.data_ptr(), g_forcing[t].data_ptr(),
-                        scratch.data_ptr()), "adj_reverse")
-            _lib.check(self.lib.cmf_adj_finalize(plan, stream, lam.data_ptr(), grad.data_ptr(),
-                                                 scratch.data_ptr()), "adj_finalize")
+                        plan, main.cuda_stream, tape.data_ptr() + j0 * stride, m,
+                        forcing[t].data_ptr(), dts[t], lam.data_ptr(), grad.data_ptr(),
+                        g_forcing[t].data_ptr(), scratch.data_ptr()), "adj_reverse")
+                free[buf].record(main)
+            _lib.check(self.lib.cmf_adj_finalize(plan, main.cuda_stream, lam.data_ptr(),
+                                                 grad.data_ptr(), scratch.data_ptr()),
+                       "adj_finalize")
+            main.wait_stream(side)
         finally:
             self.lib.cmf_adj_plan_destroy(plan)
         return grad, g_forcing, lam
