@@ -592,6 +592,22 @@ class CaMaFlood:
         _lib.check(_lib.lib().cmf_launch_substep(self._plan, self._stream(), int(k), int(part)),
                    "launch_substep")
 
+    def _rebuild_plan(self, block_size: int) -> None:
+        """Rebuild the plan (and its interval graph) with another CTA size;
+        the state lives in the model tensors between intervals, so this is
+        safe between two step_advance calls."""
+        self.close()
+        self.block_size = int(block_size)
+        self._create_plan()
+
+    def autotune_block_size(self, candidates=None, sub_steps: int = 6,
+                            cache_path: Optional[str] = None) -> dict:
+        """Measure the candidate CTA sizes on this network and keep the
+        fastest (cmfb200.autotune.tune_block_size); the state is unchanged."""
+        from .autotune import DEFAULT_CANDIDATES, tune_block_size
+        return tune_block_size(self, candidates or DEFAULT_CANDIDATES, sub_steps,
+                               cache_path=cache_path)
+
     def flush_budget(self) -> None:
         _lib.check(_lib.lib().cmf_budget_flush(self._plan, self._stream()), "budget_flush")
 
