@@ -241,21 +241,20 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
                         "plain models; includes the state reset copies of the looped runs"}
 
 
-def adjoint_compare(device, days: int, checkpoint_every: int = 96,
-                    catchments: int = 250_000) -> dict:
+def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
     """Forward+adjoint against forward on the calibration window: the
-    250k-catchment network of the full-physics config with the base physics
-    only (the adjoint covers no bifurcation, levee or reservoir), fp64, daily
-    forcing over `days` intervals, discharge at 500 cells with upstream area
-    > 1000 km^2, relative-misfit loss against a run with river Manning x
-    lognormal(0.2).  Both are timed with CUDA events on the same GPU from the
-    same spun-up state; the gradient run includes its checkpointed forward."""
+    250k-catchment full-physics network (8,000 bifurcation paths, levees on
+    20 % of cells, 500 reservoirs), fp64, daily forcing over `days`
+    intervals, discharge at 500 cells with upstream area > 1000 km^2,
+    relative-misfit loss against a run with river Manning x lognormal(0.2).
+    Both are timed with CUDA events on the same GPU from the same spun-up
+    state; the gradient run includes its checkpointed forward."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn, topology
     from cmfb200.adjoint import AdjointRouting
-    net = syn.generate(syn.NetworkSpec(catchments, seed=1, levee_fraction=0.0))
+    net = syn.generate(syn.CONFIGS["full_250k"]["spec"])
     model = CaMaFlood(device=device, input_proxy=net.fields,
-                      opened_modules=["base", "adaptive_time"], precision="float64")
+                      opened_modules=net.opened_modules, precision="float64")
     model.set_inputs(torch.as_tensor(syn.daily_runoff(net, 0)[model.order]).to(device))
     model.step_advance()
     fx = model.export_fields()
@@ -332,7 +331,7 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96,
             "catchments": n, "sub_steps": subs,
             "days": days, "checkpoint_every": checkpoint_every, "gauges": int(gauges.size),
             "dtype": "f64",
-            "workload": "base-physics 250k network, fp64, daily forcing, gradients w.r.t. "
+            "workload": "full-physics 250k network, fp64, daily forcing, gradients w.r.t. "
                         "river Manning, river height, river width and runoff; fwd = the same "
                         "primal kernels without checkpoints; product_fwd = CaMaFlood.step_advance "
                         "in fp64 (interval graphs) over the same window"}

@@ -6,15 +6,18 @@ forcing intervals through the fp64 primal kernels of libcmfb200
 its backward recomputes each checkpoint segment with a tape and sweeps it in
 reverse (`cmf_adj_reverse`).  The gradients reach the river and floodplain
 Manning coefficients, river height, river width, the runoff of every interval
-and the initial state.
+and the initial state.  Every physics module of the model is differentiated:
+base, bifurcation, levee and reservoir.
 
 The sub-step counts of the intervals come from the CFL rule on the state at
 each interval start (cmfgpu/phys/cuda/adaptive_time.cu:19-48) and carry no
 gradient, like `floor` and `.item()` in the reference's step
 (cmfgpu/models/cama_flood_model.py:119-132).
 
-State layout: a [9, N] fp64 tensor in model (breadth-first) order, field
-order `STATE`.  Parameters and forcing are model-ordered fp64 tensors.
+State: one flat fp64 tensor, model (breadth-first) order: the cell fields
+`CELL_STATE` as [12, N], then the path fields `PATH_STATE` as [2, P*L]
+(`AdjointRouting.unpack` / `pack` convert).  Parameters and forcing are
+model-ordered fp64 tensors.
 """
 from __future__ import annotations
 
@@ -25,19 +28,25 @@ import torch
 
 from . import _lib
 
-STATE = ("river_storage", "flood_storage", "river_outflow", "flood_outflow", "river_depth",
-         "flood_depth", "river_cross_section_depth", "flood_cross_section_depth",
-         "flood_cross_section_area")
+CELL_STATE = ("river_storage", "flood_storage", "river_outflow", "flood_outflow", "river_depth",
+              "flood_depth", "river_cross_section_depth", "flood_cross_section_depth",
+              "flood_cross_section_area", "protected_storage", "protected_depth",
+              "reservoir_total_inflow")
+PATH_STATE = ("bifurcation_outflow", "bifurcation_cross_section_depth")
+STATE = CELL_STATE + PATH_STATE
 PARAMS = ("river_manning", "flood_manning", "river_height", "river_width")
 F_ROUT, F_FOUT = 2, 3
+SLOT_CELL_FIELDS = 15        # the 12 cell state fields + flux, flux, limit rate
 
 
 def _bind(h) -> None:
     if getattr(h, "_adj_bound", False):
         return
     P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
-    h.cmf_adj_layout.restype = I
-    h.cmf_adj_layout.argtypes = [ctypes.POINTER(I)] * 4
+    I64 = ctypes.c_int64
+    h.cmf_adj_sizes.restype = I
+    h.cmf_adj_sizes.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64),
+                                ctypes.POINTER(I)]
     h.cmf_adj_plan_create.restype = I
     h.cmf_adj_plan_create.argtypes = [ctypes.POINTER(_lib.CmfView), ctypes.POINTER(P)]
     h.cmf_adj_plan_destroy.restype = None
@@ -56,9 +65,9 @@ def _bind(h) -> None:
 class AdjointRouting:
     """Gradient engine bound to a `CaMaFlood` model.
 
-    The model must use precision "float64", one member and the base physics
-    (modules base / adaptive_time); its topology and fixed geometry are used,
-    while the four differentiated parameters are passed per window.
+    The model must use precision "float64" and one member; its topology,
+    fixed geometry and module tables are used, while the four differentiated
+    parameters are passed per window.
 
     gauges            model-order indices of the cells whose discharge
                       (river + floodplain outflow at each interval end) the
@@ -71,30 +80,69 @@ class AdjointRouting:
             raise ValueError("the adjoint runs in fp64: build the model with precision='float64'")
         if model.num_members != 1:
             raise ValueError("the adjoint takes a single-member model")
-        if model.bifurcation is not None or model.levee is not None or model.reservoir is not None:
-            raise NotImplementedError("the adjoint covers the base physics (no bifurcation, "
-                                      "levee or reservoir modules)")
         if checkpoint_every < 1:
             raise ValueError("checkpoint_every must be >= 1")
         self.model = model
         self.device = model.device
         self.N = model.num_catchments
+        bm = model.bifurcation
+        self.P = bm.num_bifurcation_paths if bm is not None else 0
+        self.L = bm.num_bifurcation_levels if bm is not None else 0
         self.outer = model.step_seconds
         self.K = int(checkpoint_every)
         self.gauges = torch.as_tensor(gauges, dtype=torch.long, device=self.device)
         self.lib = _lib.lib()
         _bind(self.lib)
-        cnt = [ctypes.c_int() for _ in range(4)]
-        _lib.check(self.lib.cmf_adj_layout(*[ctypes.byref(c) for c in cnt]), "adj_layout")
-        self.n_state, self.n_slot, self.n_scratch, self.n_grad = (c.value for c in cnt)
-        assert self.n_state == len(STATE) and self.n_grad == len(PARAMS)
+        b = model.base
+        plan = self._plan(*(getattr(b, k).detach().contiguous() for k in PARAMS))
+        try:
+            sl, tl, sc = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+            gf = ctypes.c_int()
+            _lib.check(self.lib.cmf_adj_sizes(plan, ctypes.byref(sl), ctypes.byref(tl),
+                                              ctypes.byref(sc), ctypes.byref(gf)), "adj_sizes")
+        finally:
+            self.lib.cmf_adj_plan_destroy(plan)
+        self.state_len, self.slot_len, self.scratch_len, self.n_grad = (
+            sl.value, tl.value, sc.value, gf.value)
+        assert self.state_len == len(CELL_STATE) * self.N + 2 * self.P * self.L
+        assert self.n_grad == len(PARAMS)
+        self._cells = len(CELL_STATE) * self.N
+        self._path_off = SLOT_CELL_FIELDS * self.N
         self._n_dev = torch.zeros(1, dtype=torch.int32, device=self.device)
 
     # ------------------------------------------------------------------ #
+    def pack(self, fields: dict) -> torch.Tensor:
+        """Flat state from a dict of model-ordered tensors (missing module
+        fields are zero)."""
+        n, pl = self.N, self.P * self.L
+        out = torch.zeros(self.state_len, dtype=torch.float64, device=self.device)
+        for f, name in enumerate(CELL_STATE):
+            if name in fields:
+                out[f * n:(f + 1) * n] = fields[name].reshape(-1).to(out)
+        for f, name in enumerate(PATH_STATE):
+            if name in fields and pl:
+                out[self._cells + f * pl:self._cells + (f + 1) * pl] = fields[name].reshape(-1).to(out)
+        return out
+
+    def unpack(self, state: torch.Tensor) -> dict:
+        """Views of a flat state by field name ([N] cells, [P, L] paths)."""
+        n, pl = self.N, self.P * self.L
+        out = {name: state[f * n:(f + 1) * n] for f, name in enumerate(CELL_STATE)}
+        if pl:
+            for f, name in enumerate(PATH_STATE):
+                out[name] = state[self._cells + f * pl:self._cells + (f + 1) * pl].view(self.P, self.L)
+        return out
+
     def initial_state(self) -> torch.Tensor:
-        """The model's current state as a [9, N] fp64 tensor."""
-        b = self.model.base
-        return torch.stack([getattr(b, k).detach().to(torch.float64) for k in STATE]).contiguous()
+        """The model's current state as a flat fp64 tensor."""
+        m = self.model
+        fields = {k: getattr(m.base, k).detach() for k in CELL_STATE if hasattr(m.base, k)}
+        if m.reservoir is not None:
+            fields["reservoir_total_inflow"] = m.reservoir.reservoir_total_inflow.detach()
+        if m.bifurcation is not None:
+            for k in PATH_STATE:
+                fields[k] = getattr(m.bifurcation, k).detach()
+        return self.pack(fields)
 
     def parameters(self) -> dict[str, torch.Tensor]:
         """Copies of the model's four differentiable parameters."""
@@ -123,8 +171,22 @@ class AdjointRouting:
             raise FloatingPointError(f"CFL sub-step count {n} out of range (non-finite depth?)")
         return n
 
+    # slot <-> state copies (the slot holds the state's cell fields first and
+    # its path fields at the start of the path area)
+    def _state_to_slot(self, state, slot):
+        slot[:self._cells].copy_(state[:self._cells])
+        pl2 = 2 * self.P * self.L
+        if pl2:
+            slot[self._path_off:self._path_off + pl2].copy_(state[self._cells:])
+
+    def _slot_to_state(self, slot, state):
+        state[:self._cells].copy_(slot[:self._cells])
+        pl2 = 2 * self.P * self.L
+        if pl2:
+            state[self._cells:].copy_(slot[self._path_off:self._path_off + pl2])
+
     def window(self, params: dict, forcing: torch.Tensor, state0: torch.Tensor):
-        """Differentiable window: returns (discharge [T, G], final state [9, N])."""
+        """Differentiable window: returns (discharge [T, G], final flat state)."""
         return RoutingWindow.apply(self, params["river_manning"], params["flood_manning"],
                                    params["river_height"], params["river_width"], forcing, state0)
 
@@ -142,13 +204,15 @@ class AdjointRouting:
 
     def _forward(self, rman, fman, rh, rw, forcing, state0, keep_checkpoints=True):
         rman, fman, rh, rw, forcing, state0 = self._prep(rman, fman, rh, rw, forcing, state0)
-        N, S = self.N, self.n_slot
-        if state0.shape != (self.n_state, N) or forcing.dim() != 2 or forcing.shape[1] != N:
-            raise ValueError("state0 must be [9, N] and forcing [T, N] in model order")
+        N = self.N
+        if state0.numel() != self.state_len or forcing.dim() != 2 or forcing.shape[1] != N:
+            raise ValueError("state0 must be the flat state and forcing [T, N], model order")
+        state0 = state0.reshape(-1)
         plan = self._plan(rman, fman, rh, rw)
         try:
-            slots = torch.empty((2, S, N), dtype=torch.float64, device=self.device)
-            slots[0, :self.n_state].copy_(state0)
+            slots = torch.zeros((2, self.slot_len), dtype=torch.float64, device=self.device)
+            self._state_to_slot(state0, slots[0])
+            cur = torch.empty_like(state0)
             stream = self._stream()
             T = forcing.shape[0]
             q = torch.empty((T, self.gauges.numel()), dtype=torch.float64, device=self.device)
@@ -159,24 +223,27 @@ class AdjointRouting:
                 k = 0
                 while k < n:
                     if keep_checkpoints and g % self.K == 0:
-                        ckpts[g] = slots[0, :self.n_state].clone()
+                        self._slot_to_state(slots[0], cur)
+                        ckpts[g] = cur.clone()
                     m = min(n - k, self.K - g % self.K)
                     _lib.check(self.lib.cmf_adj_forward(plan, stream, slots.data_ptr(), m, 0,
                                                         forcing[t].data_ptr(), dt), "adj_forward")
                     if m & 1:
-                        slots[0, :self.n_state].copy_(slots[1, :self.n_state])
+                        slots[0].copy_(slots[1])
                     k += m
                     g += m
                 counts.append(n)
-                q[t] = (slots[0, F_ROUT] + slots[0, F_FOUT])[self.gauges]
-            final = slots[0, :self.n_state].clone()
+                q[t] = (slots[0, F_ROUT * N:(F_ROUT + 1) * N]
+                        + slots[0, F_FOUT * N:(F_FOUT + 1) * N])[self.gauges]
+            final = torch.empty_like(state0)
+            self._slot_to_state(slots[0], final)
         finally:
             self.lib.cmf_adj_plan_destroy(plan)
         return q, final, counts, ckpts, (rman, fman, rh, rw, forcing)
 
     def _backward(self, saved, counts, ckpts, q_bar, state_bar):
         rman, fman, rh, rw, forcing = saved
-        N, S, dev = self.N, self.n_slot, self.device
+        N, dev = self.N, self.device
         T = forcing.shape[0]
         dts = [self.outer / n for n in counts]
         starts, ends, acc = [], [], 0
@@ -185,17 +252,20 @@ class AdjointRouting:
             acc += n
             ends.append(acc)
         total = acc
-        lam = torch.zeros((self.n_state, N), dtype=torch.float64, device=dev)
+        lam = torch.zeros(self.state_len, dtype=torch.float64, device=dev)
         if state_bar is not None:
-            lam += state_bar.to(dev, torch.float64)
+            lam += state_bar.reshape(-1).to(dev, torch.float64)
+        lam_rout = lam[F_ROUT * N:(F_ROUT + 1) * N]
+        lam_fout = lam[F_FOUT * N:(F_FOUT + 1) * N]
         grad = torch.zeros((self.n_grad, N), dtype=torch.float64, device=dev)
         g_forcing = torch.zeros((T, N), dtype=torch.float64, device=dev)
-        scratch = torch.zeros((self.n_scratch, N), dtype=torch.float64, device=dev)
+        scratch = torch.zeros(self.scratch_len, dtype=torch.float64, device=dev)
         seg_len = min(self.K, max(total, 1))
         # Two tapes: segment s-1 is recomputed on a side stream while segment s
         # is swept in reverse on the caller's stream (the two are independent).
-        tapes = [torch.empty((seg_len + 1, S, N), dtype=torch.float64, device=dev) for _ in range(2)]
-        stride = S * N * 8
+        tapes = [torch.zeros((seg_len + 1, self.slot_len), dtype=torch.float64, device=dev)
+                 for _ in range(2)]
+        stride = self.slot_len * 8
         main = torch.cuda.current_stream(dev)
         side = torch.cuda.Stream(dev)
         side.wait_stream(main)
@@ -210,7 +280,7 @@ class AdjointRouting:
             tape = tapes[buf]
             chunks, g = [], g0
             with torch.cuda.stream(side):
-                tape[0, :self.n_state].copy_(ckpts[g0])
+                self._state_to_slot(ckpts[g0], tape[0])
                 while g < g1:
                     t = bisect.bisect_right(starts, g) - 1
                     m = min(g1, ends[t]) - g
@@ -237,8 +307,8 @@ class AdjointRouting:
                 for t, j0, m in reversed(chunks):
                     if q_bar is not None and g0 + j0 + m == ends[t]:
                         qb = q_bar[t].to(dev, torch.float64)
-                        lam[F_ROUT].index_add_(0, self.gauges, qb)
-                        lam[F_FOUT].index_add_(0, self.gauges, qb)
+                        lam_rout.index_add_(0, self.gauges, qb)
+                        lam_fout.index_add_(0, self.gauges, qb)
                     _lib.check(self.lib.cmf_adj_reverse(
                         plan, main.cuda_stream, tape.data_ptr() + j0 * stride, m,
                         forcing[t].data_ptr(), dts[t], lam.data_ptr(), grad.data_ptr(),
@@ -255,8 +325,8 @@ class AdjointRouting:
 
 class RoutingWindow(torch.autograd.Function):
     """(engine, river_manning, flood_manning, river_height, river_width,
-    forcing [T, N], state0 [9, N]) -> (discharge at the gauges [T, G],
-    final state [9, N]); all fp64, model order."""
+    forcing [T, N], flat initial state) -> (discharge at the gauges [T, G],
+    flat final state); all fp64, model order."""
 
     @staticmethod
     def forward(ctx, engine, rman, fman, rh, rw, forcing, state0):
@@ -265,6 +335,7 @@ class RoutingWindow(torch.autograd.Function):
         ctx.counts = counts
         ctx.ckpts = ckpts
         ctx.saved = saved
+        ctx.state_shape = state0.shape
         return q, final
 
     @staticmethod
@@ -272,4 +343,4 @@ class RoutingWindow(torch.autograd.Function):
         grad, g_forcing, lam = ctx.engine._backward(ctx.saved, ctx.counts, ctx.ckpts, q_bar,
                                                     state_bar)
         ctx.ckpts = None
-        return None, grad[0], grad[1], grad[2], grad[3], g_forcing, lam
+        return None, grad[0], grad[1], grad[2], grad[3], g_forcing, lam.view(ctx.state_shape)

@@ -1,36 +1,53 @@
-// Reverse-mode adjoint of the base-physics sub-step, fp64.
+// Reverse-mode adjoint of the routing sub-step, fp64, all physics modules.
 //
 // The reference has no adjoint; this is the differentiable routing core the
 // calibration path needs.  A forward sub-step k maps the state
 //
 //   X_k = (river/flood storage, river/flood outflow, river/flood depth,
-//          river/flood cross-section depth, flood cross-section area)
+//          river/flood cross-section depth, flood cross-section area,
+//          protected storage, protected depth, reservoir total inflow;
+//          per bifurcation path and level: outflow, cross-section depth)
 //
-// to X_{k+1} through three phases that each read neighbours (momentum reads
-// the downstream depth; the limiter and the stage read the upstream fluxes
-// and limit rates).  The primal phases here restate the product forward
-// (cmf_device.cuh, REAL = double, base physics) with every intermediate kept,
-// and a "tape" slot stores X_k plus the sub-step's fluxes and limit rates:
+// to X_{k+1} through phases that read neighbours (momentum reads the
+// downstream depth; a path reads both end cells; the limiter and the stage
+// read the upstream fluxes, the path sums and the limit rates).  The primal
+// kernels here restate the product forward (cmf_device.cuh, REAL = double)
+// with every intermediate kept, and a tape slot stores X_k with the
+// sub-step's fluxes, limit rates and limited path fluxes.
 //
-//   slot k = [X_k (9 fields) | qr, qf, lr of sub-step k] x N doubles.
+// The reverse of one sub-step is up to eight kernels, each a gather: every scatter of
+// the forward (inflow into the downstream cell, outgoing storage of the
+// downstream cell, the downstream depth read by momentum, path fluxes into
+// their end cells, reservoir inflow) becomes a gather over the contiguous
+// upstream range of the breadth-first order or over the per-cell path CSR, so
+// the adjoint is deterministic and atomic-free like the forward:
 //
-// The reverse of one sub-step is three per-cell kernels; every scatter of the
-// forward (inflow into the downstream cell, outgoing storage of the downstream
-// cell, the downstream depth read by momentum) becomes a gather over the
-// contiguous upstream range of the breadth-first order, so the adjoint is
-// deterministic and atomic-free like the forward:
+//   kr_levee       levee re-partition reversed over the levee list, one
+//                  thread per levee and input direction;
+//   kr_stage       flood stage and storage update reversed per cell, after
+//                  the pending depth/storage adjoints that the later
+//                  sub-step's momentum and path kernels left behind;
+//   kr_stage_path  path inflow (net flux, level-flux scaling) reversed;
+//   kr_limit       limit-rate and outgoing-storage adjoints;
+//   kr_momentum    local-inertial momentum reversed per cell;
+//   kr_dam         reservoir release and the dam-upstream kinematic flow
+//                  reversed for the dam cells;
+//   kr_path        path momentum reversed, one thread per path and input
+//                  direction.
 //
-//   kr_stage     flood stage and storage update reversed per cell (plus the
-//                pending downstream-depth adjoints of the upstream cells);
-//   kr_limit     limit-rate adjoint gathered over the cell, its upstream cells
-//                and its downstream cell; outgoing-storage adjoint;
-//   kr_momentum  local-inertial momentum reversed per cell; writes lambda_k
-//                and accumulates the parameter gradients.
+// The long scalar branches -- reservoir release, dam-upstream kinematic flow,
+// path momentum with its limiter, levee re-partition -- are templates on the
+// scalar type.  The primal evaluates them on double; the reverse evaluates
+// them on a forward-mode dual number, one input direction at a time, and
+// contracts the Jacobian columns with the output adjoints.  The local-inertial
+// momentum and the flood stage are reversed by hand.
 //
-// The subgradient convention is that of the PyTorch transcription used as
-// the autograd oracle: clamp passes the gradient on its bounds, a two-operand
-// max splits it at a tie, a ternary routes it to the taken branch, and
-// max(sqrt(p), f) is differentiable only where p > f*f.
+// Subgradient convention (that of the PyTorch transcription used as the
+// autograd oracle): clamp passes the gradient on its bounds, a two-operand
+// max of the momentum splits it at a tie, a ternary routes it to the taken
+// branch, max(sqrt(p), f) is differentiable only where p > f*f; in the
+// templated branches fmax/fmin take the first operand on a tie and sqrt/cbrt
+// have derivative 0 at 0.
 
 #include "cmfb200.h"
 
@@ -41,24 +58,117 @@
 
 namespace {
 
-enum StateField { F_RS = 0, F_FS, F_ROUT, F_FOUT, F_RDEP, F_FDEP, F_RCSD, F_FCSD, F_FCSA,
-                  kStateFields };
-enum SlotExtra { F_QR = kStateFields, F_QF, F_LR, kSlotFields };
-enum Scratch { S_RINB = 0, S_FINB, S_ROB, S_FOB, S_OGB, S_QRB, S_QFB, S_WDNB, kScratchFields };
+// ---------------------------------------------------------------------------
+// layout
+// ---------------------------------------------------------------------------
+enum CellField { F_RS = 0, F_FS, F_ROUT, F_FOUT, F_RDEP, F_FDEP, F_RCSD, F_FCSD, F_FCSA, F_PS,
+                 F_PDEP, F_RTI, kCellState };
+enum SlotExtra { F_QR = kCellState, F_QF, F_LR, kSlotCell };
+// path area of a slot: [BOUT | BCSD | BLIM] x P*L, then [BSUM | BRAW] x P
+enum PathField { PF_BOUT = 0, PF_BCSD, PF_BLIM };
+// cell scratch of the reverse sweep
+enum Scratch { S_RINB = 0, S_FINB, S_ROB, S_FOB, S_OGB, S_QRB, S_QFB, S_WDNB, S_GBB, S_RTIB,
+               kCellScratch };
+// path scratch: [LRCB | LRDB] x P, BLIMB x P*L, PEB x 6P
 enum Grad { G_RMAN = 0, G_FMAN, G_RH, G_RW, kGradFields };
 
 constexpr int kBlock = 256;
+constexpr int kMaxLevels = 8;
+constexpr int kMaxFloodLevels = 16;
 constexpr double kFloor = 1e-6;
 constexpr double kFloor2 = 1e-6 * 1e-6;
 
+// ---------------------------------------------------------------------------
+// forward-mode dual number
+// ---------------------------------------------------------------------------
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual D(double v) { return {v, 0.0}; }
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b)
+{
+    const double q = a.v / b.v;
+    return {q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__device__ __forceinline__ Dual operator/(double a, Dual b)
+{
+    const double q = a / b.v;
+    return {q, -q * b.d / b.v};
+}
+
+__device__ __forceinline__ double val(double x) { return x; }
+__device__ __forceinline__ double val(Dual x) { return x.v; }
+__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ double vmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ Dual vmax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
+__device__ __forceinline__ Dual vmin(Dual a, Dual b) { return a.v <= b.v ? a : b; }
+__device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ Dual vsqrt(Dual a)
+{
+    const double s = sqrt(a.v);
+    return {s, a.v > 0.0 ? a.d / (2.0 * s) : 0.0};
+}
+__device__ __forceinline__ double vcbrt(double a) { return cbrt(a); }
+__device__ __forceinline__ Dual vcbrt(Dual a)
+{
+    const double c = cbrt(a.v);
+    return {c, a.v != 0.0 ? a.d / (3.0 * c * c) : 0.0};
+}
+__device__ __forceinline__ double vexp(double a) { return exp(a); }
+__device__ __forceinline__ Dual vexp(Dual a)
+{
+    const double e = exp(a.v);
+    return {e, e * a.d};
+}
+__device__ __forceinline__ double vlog(double a) { return log(a); }
+__device__ __forceinline__ Dual vlog(Dual a) { return {log(a.v), a.d / a.v}; }
+__device__ __forceinline__ double vabs(double a) { return fabs(a); }
+__device__ __forceinline__ Dual vabs(Dual a)
+{
+    return {fabs(a.v), (double)((a.v > 0.0) - (a.v < 0.0)) * a.d};
+}
+template <typename T>
+__device__ __forceinline__ T cnst(double x) { return T(x); }
+template <>
+__device__ __forceinline__ Dual cnst<Dual>(double x) { return D(x); }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
 struct Ctx {
-    long N;
-    int K;
-    double g, alpha, max_dt;
+    long N, P;
+    int K, L;
+    bool lev, res, bif;
+    double g, alpha, max_dt, min_kin;
     const int* dn;
     const int* up;
     const uint8_t* flags;
     const double *rw, *rl, *rh, *celv, *ca, *dnd, *rman, *fman, *tbl;
+    // levee (slot per cell, cell per slot)
+    long NLV, R;
+    const int* lslot;
+    const int* lci;
+    const int* rci;
+    const double *lcrown, *lfrac, *lbase;
+    // reservoir (slot per cell)
+    const int* rslot;
+    const double *rcons, *remerg, *radj, *rnout, *raout, *rfcout;
+    // bifurcation
+    const int *bptr, *bpaths, *bci, *bdi;
+    const double *bman, *bwid, *blen, *belv;
+    // slot geometry (doubles)
+    long slot_len, path_off;
+    int grid_cells, grid_paths;
 };
 
 __device__ __forceinline__ int up_end(const Ctx& c, long x)
@@ -69,9 +179,289 @@ __device__ __forceinline__ int up_end(const Ctx& c, long x)
 
 __device__ __forceinline__ double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
 
+// path-area accessors of a slot
+__device__ __forceinline__ double* pth(const Ctx& c, double* X, int f) { return X + c.path_off + (long)f * c.P * c.L; }
+__device__ __forceinline__ const double* pth(const Ctx& c, const double* X, int f) { return X + c.path_off + (long)f * c.P * c.L; }
+__device__ __forceinline__ double* bsum_of(const Ctx& c, double* X) { return X + c.path_off + 3L * c.P * c.L; }
+__device__ __forceinline__ const double* bsum_of(const Ctx& c, const double* X) { return X + c.path_off + 3L * c.P * c.L; }
+__device__ __forceinline__ double* braw_of(const Ctx& c, double* X) { return bsum_of(c, X) + c.P; }
+__device__ __forceinline__ const double* braw_of(const Ctx& c, const double* X) { return bsum_of(c, X) + c.P; }
+
 // ---------------------------------------------------------------------------
-// Momentum primal with its intermediates (outflow.cu:21-135, base physics; the
-// same operation order as momentum_cell with REAL = double).
+// templated scalar branches
+// ---------------------------------------------------------------------------
+
+// Reservoir release (reservoir.cu:18-94).
+template <typename T>
+__device__ __forceinline__ T release(const Ctx& c, int slot, T rs, T fs, T total_inflow, T runoff_v,
+                                     double time_step)
+{
+    T total = rs + fs;
+    T inflow = total_inflow + runoff_v;
+    const double cons = c.rcons[slot], emerg = c.remerg[slot], adj = c.radj[slot];
+    const double n_out = c.rnout[slot], a_out = c.raout[slot], fc_out = c.rfcout[slot];
+    T ro;
+    if (val(total) <= cons) {
+        ro = n_out * vsqrt(total / cons);
+    } else if (val(total) <= adj) {
+        T frac2 = (total - cons) / (adj - cons);
+        ro = n_out + vexp(3.0 * vlog(frac2)) * (a_out - n_out);
+    } else if (val(total) <= emerg) {
+        T frac3 = (total - adj) / (emerg - adj);
+        T tmp = a_out + vexp(0.1 * vlog(frac3)) * (fc_out - a_out);
+        if (val(inflow) >= fc_out) {
+            T flood = n_out + ((total - cons) / (emerg - cons)) * (inflow - n_out);
+            ro = vmax(flood, tmp);
+        } else {
+            ro = tmp;
+        }
+    } else {
+        ro = (val(inflow) >= fc_out) ? inflow : cnst<T>(fc_out);
+    }
+    ro = vmax(ro, cnst<T>(0.0));
+    ro = vmin(ro, total / time_step);
+    return ro;
+}
+
+// Kinematic flow of a cell right upstream of a dam (outflow.cu:137-153).
+template <typename T>
+__device__ __forceinline__ void kinematic(const Ctx& c, long i, T r_dep, T f_dep, T rs, T fs, T r_wid,
+                                          T r_man, T f_man, double time_step, T& kin_riv, T& kin_fld)
+{
+    const int dn = c.dn[i];
+    double bed_slope = (c.celv[i] - c.celv[dn]) / c.dnd[i];
+    bed_slope = fmax(bed_slope, c.min_kin);
+    T kin_riv_vel = (1.0 / r_man) * sqrt(bed_slope) * vcbrt(r_dep * r_dep);
+    kin_riv = r_wid * r_dep * kin_riv_vel;
+    kin_riv = vmin(kin_riv, rs / time_step);
+    kin_riv = vmax(kin_riv, cnst<T>(0.0));
+    const double bed_slope_f = fmin(bed_slope, 0.005);
+    T kin_fld_vel = (1.0 / f_man) * sqrt(bed_slope_f) * vcbrt(f_dep * f_dep);
+    T kin_fld_area = vmax(fs / c.rl[i] - f_dep * r_wid, cnst<T>(0.0));
+    kin_fld = kin_fld_area * kin_fld_vel;
+    kin_fld = vmin(kin_fld, fs / time_step);
+    kin_fld = vmax(kin_fld, cnst<T>(0.0));
+}
+
+// Path momentum with the path limiter (bifurcation.cu:21-129,
+// levee.cu:263-341): in = (wse_c, wse_d, pwse_c, pwse_d, tot_c, tot_d,
+// outflow[L], cross-section depth[L]); out = limited level fluxes, their
+// limited sum and the new cross-section depths.
+template <typename T>
+__device__ __forceinline__ void path_flux(const Ctx& c, long p, const T* in, double time_step,
+                                          T* blim, T& bsum, T* bcsd_new)
+{
+    const int L = c.L;
+    const T wse_c = in[0], wse_d = in[1], pwse_c = in[2], pwse_d = in[3];
+    const T ts_c = in[4], ts_d = in[5];
+    const double gravity = c.g;
+    const double blen = c.blen[p];
+    T max_wse = vmax(wse_c, wse_d);
+    T max_pwse = vmax(pwse_c, pwse_d);
+    T slope = (wse_c - wse_d) / blen;
+    slope = vmin(vmax(slope, cnst<T>(-0.005)), cnst<T>(0.005));
+    T upd[kMaxLevels];
+    T sum_out = cnst<T>(0.0);
+    for (int lv = 0; lv < L; ++lv) {
+        const long lp = p * (long)L + lv;
+        const double elv = c.belv[lp];
+        const T o = in[6 + lv];
+        const T csd = in[6 + L + lv];
+        T upd_csd, sifd;
+        if (c.lev) {
+            T current_max_wse = (lv == 0) ? max_wse : max_pwse;
+            upd_csd = vmax(current_max_wse - elv, cnst<T>(0.0));
+            if (lv == 0) {
+                sifd = vsqrt(upd_csd * csd);
+                if (val(sifd) <= 0.0) sifd = upd_csd;
+            } else {
+                sifd = upd_csd;
+            }
+        } else {
+            upd_csd = vmax(max_wse - elv, cnst<T>(0.0));
+            sifd = vmax(vsqrt(upd_csd * csd), vsqrt(upd_csd * 0.01));
+        }
+        T upd_o = cnst<T>(0.0);
+        if (val(sifd) > 1e-5) {
+            const double man = c.bman[lp];
+            const double w = c.bwid[lp];
+            T unit_o = o / w;
+            T num = w * (unit_o + gravity * time_step * sifd * slope);
+            T den = 1.0 + gravity * time_step * (man * man) * vabs(unit_o)
+                    * (1.0 / (sifd * sifd * vcbrt(sifd)));
+            upd_o = num / den;
+        }
+        sum_out = sum_out + upd_o;
+        bcsd_new[lv] = upd_csd;
+        upd[lv] = upd_o;
+    }
+    T lr_p = cnst<T>(1.0);
+    const double denom = fabs(val(sum_out)) * time_step;
+    if (denom > 0.0) lr_p = vmin(0.05 * vmin(ts_c, ts_d) / (vabs(sum_out) * time_step), cnst<T>(1.0));
+    bsum = sum_out * lr_p;
+    for (int lv = 0; lv < L; ++lv) blim[lv] = upd[lv] * lr_p;
+}
+
+// Levee re-partition (levee.cu:29-261) of a levee cell after its flood stage.
+// in = (river storage, flood storage, river depth, flood depth, river width,
+// river height); out = (river, flood, protected storage, river, flood,
+// protected depth); the flooded fraction passes through `ffr` (value only).
+template <typename T>
+__device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, double& ffr, T* out)
+{
+    const int slot = c.lslot[ci];
+    const int nl = c.K;
+    const double rl = c.rl[ci], ca = c.ca[ci];
+    const double l_crown = c.lcrown[slot], l_frac = c.lfrac[slot], l_base_h = c.lbase[slot];
+    const T riv_sto_curr = in[0], fld_sto_curr = in[1];
+    const T total_sto = riv_sto_curr + fld_sto_curr;
+    const T r_dep_curr = in[2], fld_depth_curr = in[3], rw = in[4], rh = in[5];
+    T riv_max_sto = rl * rw * rh;
+    if (!(val(total_sto) >= val(riv_max_sto))) {
+        out[0] = riv_sto_curr;
+        out[1] = fld_sto_curr;
+        out[2] = cnst<T>(0.0);
+        out[3] = r_dep_curr;
+        out[4] = fld_depth_curr;
+        out[5] = cnst<T>(0.0);
+        return;
+    }
+    const double dwth_inc = (ca / rl) / (double)nl;
+    const double levee_dist = l_frac * (ca / rl);
+    T s_curr = riv_max_sto;
+    double dhgt_pre = 0.0;
+    T dwth_pre = rw;
+    T levee_base_sto = riv_max_sto;
+    T levee_fill_sto = riv_max_sto;
+    bool found_base = false, found_fill = false;
+    const int ilev = (int)(l_frac * (double)nl);
+    T dsto_fil_B = cnst<T>(0.0), dwth_fil_B = cnst<T>(0.0);
+    double ddph_fil_B = 0.0, gradient_B = 0.0;
+    bool found_B = false;
+    bool scan_needed = true;
+    const double* row = c.tbl + ci * (long)nl;
+    for (int l = 0; l < nl; ++l) {
+        if (!scan_needed) break;
+        const double depth_val = row[l];
+        const double dhgt_seg = fmax(depth_val - dhgt_pre, 1e-6);
+        T dwth_mid = dwth_pre + 0.5 * dwth_inc;
+        T dsto_seg = rl * dwth_mid * dhgt_seg;
+        T s_next = s_curr + dsto_seg;
+        const double gradient = dhgt_seg / dwth_inc;
+
+        const bool cond_base = (l_base_h > dhgt_pre) && (l_base_h <= depth_val);
+        const double ratio_base = (l_base_h - dhgt_pre) / dhgt_seg;
+        T dsto_base_p = rl * (dwth_pre + 0.5 * ratio_base * dwth_inc) * (ratio_base * dhgt_seg);
+        if (cond_base && !found_base) levee_base_sto = s_curr + dsto_base_p;
+        found_base = found_base || cond_base;
+
+        const bool cond_fill = (l_crown > dhgt_pre) && (l_crown <= depth_val);
+        const double ratio_fill = (l_crown - dhgt_pre) / dhgt_seg;
+        T dsto_fill_p = rl * (dwth_pre + 0.5 * ratio_fill * dwth_inc) * (ratio_fill * dhgt_seg);
+        if (cond_fill && !found_fill) levee_fill_sto = s_curr + dsto_fill_p;
+        found_fill = found_fill || cond_fill;
+
+        const double dhgt_dif_loop = l_crown - l_base_h;
+        T s_top_loop = levee_base_sto + (levee_dist + rw) * dhgt_dif_loop * rl;
+        T dsto_add_wedge = (levee_dist + rw) * (l_crown - depth_val) * rl;
+        T threshold = s_next + dsto_add_wedge;
+
+        const bool cond_check = (l >= ilev) && !found_B;
+        const bool cond_found = cond_check && (val(total_sto) < val(threshold));
+        T current_lb = (l == ilev) ? s_top_loop : dsto_fil_B;
+        if (cond_check && !cond_found) {
+            dsto_fil_B = threshold;
+            dwth_fil_B = cnst<T>(dwth_inc * (double)(l + 1) - levee_dist);
+            ddph_fil_B = depth_val - l_base_h;
+        } else {
+            dsto_fil_B = current_lb;
+        }
+        if (cond_found) gradient_B = gradient;
+        found_B = found_B || cond_found;
+
+        s_curr = s_next;
+        dhgt_pre = depth_val;
+        dwth_pre = dwth_pre + dwth_inc;
+        scan_needed = !(found_base && found_fill && found_B);
+    }
+    T s_base_extra = s_curr + rl * dwth_pre * (l_base_h - dhgt_pre);
+    if (!found_base) levee_base_sto = (l_base_h > dhgt_pre) ? s_base_extra : riv_max_sto;
+    T s_fill_extra = s_curr + rl * dwth_pre * (l_crown - dhgt_pre);
+    if (!found_fill) levee_fill_sto = (l_crown > dhgt_pre) ? s_fill_extra : riv_max_sto;
+
+    const double dhgt_dif = l_crown - l_base_h;
+    T s_top = levee_base_sto + (levee_dist + rw) * dhgt_dif * rl;
+    const bool is_case4 = val(total_sto) >= val(levee_fill_sto);
+    const bool is_case3 = (!is_case4) && (val(total_sto) >= val(s_top));
+    const bool is_case2 = (!is_case4) && (!is_case3) && (val(total_sto) >= val(levee_base_sto));
+
+    T dsto_add_c2 = total_sto - levee_base_sto;
+    T dwth_add_c2 = levee_dist + rw;
+    T f_dph_c2 = l_base_h + dsto_add_c2 / dwth_add_c2 / rl;
+    T r_sto_c2 = riv_max_sto + rl * rw * f_dph_c2;
+    T r_dph_c2 = r_sto_c2 / rl / rw;
+    T f_sto_c2 = vmax(total_sto - r_sto_c2, cnst<T>(0.0));
+    const double f_frc_c2 = l_frac;
+
+    T dsto_add_B = total_sto - dsto_fil_B;
+    T term_B = dwth_fil_B * dwth_fil_B + 2.0 * dsto_add_B / rl / (gradient_B + 1e-9);
+    T dwth_add_B = -dwth_fil_B + vsqrt(vmax(term_B, cnst<T>(0.0)));
+    T ddph_add_B = dwth_add_B * gradient_B;
+    T p_dph_B_found = l_base_h + ddph_fil_B + ddph_add_B;
+    const double f_frc_B_found = (val(dwth_fil_B) + levee_dist) / (dwth_inc * (double)nl);
+    T ddph_add_B_extra = dsto_add_B / (dwth_fil_B * rl + 1e-9);
+    T p_dph_B_extra = l_base_h + ddph_fil_B + ddph_add_B_extra;
+    T p_dph_B = found_B ? p_dph_B_found : p_dph_B_extra;
+    const double f_frc_B = found_B ? f_frc_B_found : 1.0;
+
+    T r_sto_c3 = riv_max_sto + rl * rw * l_crown;
+    T r_dph_c3 = r_sto_c3 / rl / rw;
+    T f_sto_c3 = vmax(s_top - r_sto_c3, cnst<T>(0.0));
+    const double f_frc_c3 = fmin(fmax(f_frc_B, 0.0), 1.0);
+
+    T f_dph_c4 = fld_depth_curr;
+    T dsto_add_c4 = (f_dph_c4 - l_crown) * (levee_dist + rw) * rl;
+    T f_sto_c4 = vmax(s_top + dsto_add_c4 - riv_sto_curr, cnst<T>(0.0));
+
+    T r_sto_candidate = is_case2 ? r_sto_c2 : (is_case3 ? r_sto_c3 : riv_sto_curr);
+    T f_sto_candidate = is_case2 ? f_sto_c2 : (is_case3 ? f_sto_c3 : (is_case4 ? f_sto_c4 : fld_sto_curr));
+    const bool no_levee_partition = !is_case2 && !is_case3 && !is_case4;
+    T r_sto = (is_case4 || no_levee_partition) ? riv_sto_curr : vmin(r_sto_candidate, total_sto);
+    T remaining_sto = total_sto - r_sto;
+    remaining_sto = val(remaining_sto) > 0.0 ? remaining_sto : cnst<T>(0.0);
+    T f_sto = vmin(val(f_sto_candidate) > 0.0 ? f_sto_candidate : cnst<T>(0.0), remaining_sto);
+    if (is_case2) f_sto = remaining_sto;
+    if (no_levee_partition) f_sto = fld_sto_curr;
+    T p_sto = remaining_sto - f_sto;
+    p_sto = val(p_sto) > 0.0 ? p_sto : cnst<T>(0.0);
+    out[0] = r_sto;
+    out[1] = f_sto;
+    out[2] = p_sto;
+    out[3] = is_case2 ? r_dph_c2 : (is_case3 ? r_dph_c3 : r_dep_curr);
+    out[4] = is_case2 ? f_dph_c2 : (is_case3 ? cnst<T>(l_crown) : fld_depth_curr);
+    out[5] = is_case2 ? cnst<T>(0.0) : (is_case3 ? p_dph_B : (is_case4 ? f_dph_c4 : cnst<T>(0.0)));
+    ffr = is_case2 ? f_frc_c2 : (is_case3 ? f_frc_c3 : ffr);
+}
+
+// Contract the Jacobian of a templated branch with output adjoints:
+// in_bar[j] += sum_o out_bar[o] * d out[o] / d in[j], one dual pass per input.
+template <int NI, int NO, typename F>
+__device__ __forceinline__ void vjp(const double* in, const double* out_bar, double* in_bar, F f)
+{
+    for (int j = 0; j < NI; ++j) {
+        Dual x[NI];
+        for (int q = 0; q < NI; ++q) x[q] = {in[q], q == j ? 1.0 : 0.0};
+        Dual y[NO];
+        f(x, y);
+        double s = 0.0;
+        for (int o = 0; o < NO; ++o) s += out_bar[o] * y[o].d;
+        in_bar[j] += s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Momentum primal with its intermediates (outflow.cu:21-135; the same
+// operation order as momentum_cell with REAL = double).
 // ---------------------------------------------------------------------------
 struct Mom {
     bool mouth, rc, fc, zero_f, neg;
@@ -156,13 +546,64 @@ __device__ __forceinline__ void mom_eval(const Ctx& c, const double* X, long i, 
     m.tnf = 1.0;
     if (m.neg) {
         const double rs = X[F_RS * N + i];
-        const double total_storage_f = rs + fs;
+        const double ps = X[F_PS * N + i];
+        const double total_storage_f = rs + fs + ps;
         m.tnf = (-m.qr0 - m.qf1) * dt;
         m.lrn_raw = 0.05 * total_storage_f / m.tnf;
         m.lrn = fmin(m.lrn_raw, 1.0);
         m.qr = m.qr0 * m.lrn;
         m.qf = m.qf1 * m.lrn;
     }
+}
+
+// Final fluxes of a cell: momentum, then the dam-upstream and reservoir overrides.
+__device__ __forceinline__ void cell_flux(const Ctx& c, const double* X, const double* runoff, long i,
+                                          double dt, const Mom& m, double& qr, double& qf)
+{
+    const long N = c.N;
+    qr = m.qr;
+    qf = m.qf;
+    if (!c.res) return;
+    const uint8_t fl = c.flags[i];
+    if (fl & CMF_CELL_DAM_UPSTREAM) {
+        kinematic<double>(c, i, X[F_RDEP * N + i], X[F_FDEP * N + i], X[F_RS * N + i],
+                          X[F_FS * N + i], c.rw[i], c.rman[i], c.fman[i], dt, qr, qf);
+    }
+    if (fl & CMF_CELL_RESERVOIR) {
+        qr = release<double>(c, c.rslot[i], X[F_RS * N + i], X[F_FS * N + i], X[F_RTI * N + i],
+                             runoff[i], dt);
+        qf = 0.0;
+    }
+}
+
+// End state of a path end cell: water-surface elevation, protected WSE and
+// total storage (path_end_state of the product).
+__device__ __forceinline__ void end_state(const Ctx& c, const double* X, int ci, double& wse,
+                                          double& pwse, double& tot)
+{
+    const long N = c.N;
+    const uint8_t fl = c.flags[ci];
+    wse = X[F_RDEP * N + ci] + (c.celv[ci] - c.rh[ci]);
+    pwse = wse;
+    if (c.lev && (fl & CMF_CELL_LEVEE)) pwse = fmin(c.celv[ci] + X[F_PDEP * N + ci], wse);
+    const double rs = X[F_RS * N + ci], fs = X[F_FS * N + ci];
+    if (c.res && (fl & CMF_CELL_RESERVOIR)) tot = rs + fs;
+    else tot = rs + fs + X[F_PS * N + ci];
+}
+
+__device__ __forceinline__ int path_inputs(const Ctx& c, const double* X, long p, double* in)
+{
+    const int ci = c.bci[p], di = c.bdi[p];
+    end_state(c, X, ci, in[0], in[2], in[4]);
+    end_state(c, X, di, in[1], in[3], in[5]);
+    const int L = c.L;
+    const double* bout = pth(c, X, PF_BOUT);
+    const double* bcsd = pth(c, X, PF_BCSD);
+    for (int lv = 0; lv < L; ++lv) {
+        in[6 + lv] = bout[p * L + lv];
+        in[6 + L + lv] = bcsd[p * L + lv];
+    }
+    return 6 + 2 * L;
 }
 
 // ---------------------------------------------------------------------------
@@ -244,39 +685,106 @@ __device__ __forceinline__ void stage_eval(const Ctx& c, long i, double total_s,
     s.fs = flood;
 }
 
+// Reverse of stage_eval: output adjoints (river/flood storage, river/flood
+// depth) -> total-storage adjoint, plus the river width/height gradients.
+__device__ __forceinline__ double stage_reverse(const Stage& s, double tot, double rw, double rh,
+                                                double rl, double L_rs, double L_fs, double L_rdep,
+                                                double L_fdep, double& g_rw, double& g_rh)
+{
+    double tot_bar = 0.0;
+    const double rlrw = rl * rw;
+    const double rs_out_bar = L_rs + L_rdep / rlrw;       // rdep' = rs' / (rl rw)
+    g_rw += -L_rdep * s.rdep / rw;
+    if (!s.flooded) return tot_bar + rs_out_bar;
+    double river_bar = rs_out_bar;
+    if (!(tot - s.rs < 0.0)) {          // flood' = tot - river where that is >= 0
+        tot_bar += L_fs;
+        river_bar -= L_fs;
+    }
+    double cap_bar = 0.0;
+    if (s.cap_taken) cap_bar = river_bar;
+    else tot_bar += river_bar;
+    double rmax_bar = cap_bar;
+    g_rw += cap_bar * rl * s.fdep;
+    const double fdep_bar = L_fdep + cap_bar * rlrw;
+    double excess_bar, W_bar;
+    if (s.top) {
+        const double wr = s.W_tot * rl;
+        excess_bar = fdep_bar / wr;
+        W_bar = -fdep_bar * s.excess / (s.W_tot * wr);
+    } else {
+        const double dw_bar = fdep_bar * s.grad;
+        const double arg_bar = dw_bar / (2.0 * s.sq);
+        W_bar = arg_bar * 2.0 * s.W_tot - dw_bar;
+        excess_bar = arg_bar * 2.0 / (s.grad * rl);
+    }
+    tot_bar += excess_bar;
+    const double Sp_bar = -excess_bar;
+    g_rw += W_bar;
+    // S_prev = rmax + sum_{l < level} rl (W_{l-1} + W_l)/2 (H_l - H_{l-1}); the
+    // river-width derivative of the layer sum telescopes to rl * H_{level-1}
+    rmax_bar += Sp_bar;
+    if (s.level > 0) g_rw += Sp_bar * rl * s.D_prev;
+    g_rw += rmax_bar * rl * rh;
+    g_rh += rmax_bar * rlrw;
+    return tot_bar;
+}
+
 // Storage update (storage.cu:67-116) with its branch record.
 struct Store {
     double rsu1, fsu1, rsu2, tt, total_next;
-    double rin, fin, ur, uf;
+    double rin, fin, rti, gb, ur, uf;
 };
 
-// Inflow gather and own limited flux of cell i.
+// Inflow gather, own limited flux, reservoir inflow and bifurcation net flux.
 __device__ __forceinline__ void gather_inflow(const Ctx& c, const double* X, long i, Store& t)
 {
     const long N = c.N;
     const double lr_i = X[F_LR * N + i];
     const double qr = X[F_QR * N + i], qf = X[F_QF * N + i];
-    double rin = 0.0, fin = 0.0;
+    const uint8_t fl = c.flags[i];
+    const bool res_cell = c.res && (fl & CMF_CELL_RESERVOIR);
+    double rin = 0.0, fin = 0.0, rti = 0.0;
     const int c0 = c.up[i], c1 = up_end(c, i);
     for (int u = c0; u < c1; ++u) {
         const double cr = X[F_QR * N + u], cf = X[F_QF * N + u], cl = X[F_LR * N + u];
-        rin += (cr >= 0.0) ? cr * cl : cr * lr_i;
-        fin += (cf >= 0.0) ? cf * cl : cf * lr_i;
+        const double ur = (cr >= 0.0) ? cr * cl : cr * lr_i;
+        const double uf = (cf >= 0.0) ? cf * cl : cf * lr_i;
+        rin += ur;
+        fin += uf;
+        if (res_cell) rti += ur + uf;
     }
-    const bool mouth = c.flags[i] & CMF_CELL_MOUTH;
+    const bool mouth = fl & CMF_CELL_MOUTH;
     const double lr_dn = mouth ? lr_i : X[F_LR * N + c.dn[i]];
     t.rin = rin;
     t.fin = fin;
+    t.rti = rti;
     t.ur = (qr >= 0.0) ? qr * lr_i : qr * lr_dn;
     t.uf = (qf >= 0.0) ? qf * lr_i : qf * lr_dn;
+    double gb = 0.0;
+    if (c.bif && (fl & CMF_CELL_BIFURCATION)) {
+        const double* braw = braw_of(c, X);
+        for (int b = c.bptr[i]; b < c.bptr[i + 1]; ++b) {
+            const int e = c.bpaths[b];
+            const int p = e >> 1;
+            const double raw = braw[p];
+            const int other = (e & 1) ? c.bci[p] : c.bdi[p];
+            const double lr_o = X[F_LR * N + other];
+            const double lr_c = (e & 1) ? lr_o : lr_i;
+            const double lr_d = (e & 1) ? lr_i : lr_o;
+            const double net = (raw >= 0.0) ? raw * lr_c : raw * lr_d;
+            gb += (e & 1) ? -net : net;
+        }
+    }
+    t.gb = gb;
 }
 
-__device__ __forceinline__ double store_eval(const double rsto, const double fsto,
-                                             const double ro, double dt, Store& t)
+__device__ __forceinline__ double store_eval(double rsto, double fsto, double prot, double ro,
+                                             double dt, Store& t)
 {
     const double river_delta = (t.rin - t.ur) * dt;
     t.rsu1 = rsto + river_delta;
-    const double flood_delta = (t.fin - t.uf - 0.0) * dt;
+    const double flood_delta = (t.fin - t.uf - t.gb) * dt;
     t.fsu1 = fsto + (t.rsu1 < 0.0 ? t.rsu1 : 0.0) + flood_delta;
     t.rsu2 = t.rsu1 > 0.0 ? t.rsu1 : 0.0;
     double river_su = t.rsu2;
@@ -284,25 +792,68 @@ __device__ __forceinline__ double store_eval(const double rsto, const double fst
     if (t.fsu1 < 0.0) river_su = t.tt > 0.0 ? t.tt : 0.0;
     const double flood_su = t.fsu1 > 0.0 ? t.fsu1 : 0.0;
     const double external_delta = ro * dt;
-    t.total_next = river_su + flood_su + 0.0 + external_delta;
+    t.total_next = river_su + flood_su + prot + external_delta;
     return t.total_next > 0.0 ? t.total_next : 0.0;
 }
 
 // ---------------------------------------------------------------------------
 // forward kernels (tape)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) ka_momentum(const Ctx c, double* X, double* Y, double dt)
+__global__ void __launch_bounds__(kBlock) ka_momentum(const Ctx c, double* X, double* Y,
+                                                      const double* runoff, double dt)
 {
+    if ((int)blockIdx.x >= c.grid_cells) {
+        const long p = (long)(blockIdx.x - c.grid_cells) * blockDim.x + threadIdx.x;
+        if (p >= c.P) return;
+        double in[6 + 2 * kMaxLevels], blim[kMaxLevels], bcsd_new[kMaxLevels], bsum;
+        path_inputs(c, X, p, in);
+        path_flux<double>(c, p, in, dt, blim, bsum, bcsd_new);
+        double* lim = pth(c, X, PF_BLIM);
+        double* ncsd = pth(c, Y, PF_BCSD);
+        double raw = 0.0;
+        for (int lv = 0; lv < c.L; ++lv) {
+            lim[p * c.L + lv] = blim[lv];
+            ncsd[p * c.L + lv] = bcsd_new[lv];
+            raw += blim[lv];
+        }
+        bsum_of(c, X)[p] = bsum;
+        braw_of(c, X)[p] = raw;
+        return;
+    }
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
     Mom m;
     mom_eval(c, X, i, dt, m);
+    double qr, qf;
+    cell_flux(c, X, runoff, i, dt, m, qr, qf);
     const long N = c.N;
-    X[F_QR * N + i] = m.qr;
-    X[F_QF * N + i] = m.qf;
+    X[F_QR * N + i] = qr;
+    X[F_QF * N + i] = qf;
     Y[F_RCSD * N + i] = m.ucsd;
     Y[F_FCSD * N + i] = m.ufcsd;
     Y[F_FCSA * N + i] = m.ufcsa;
+}
+
+__device__ __forceinline__ double outgoing(const Ctx& c, const double* X, long i, double dt)
+{
+    const long N = c.N;
+    const double qr = X[F_QR * N + i], qf = X[F_QF * N + i];
+    double og = (fmax(qr, 0.0) + fmax(qf, 0.0)) * dt;
+    const int c0 = c.up[i], c1 = up_end(c, i);
+    for (int u = c0; u < c1; ++u) {
+        const double neg = fmin(X[F_QR * N + u], 0.0) + fmin(X[F_QF * N + u], 0.0);
+        og += -neg * dt;
+    }
+    if (c.bif && (c.flags[i] & CMF_CELL_BIFURCATION)) {
+        const double* bsum = bsum_of(c, X);
+        for (int b = c.bptr[i]; b < c.bptr[i + 1]; ++b) {
+            const int e = c.bpaths[b];
+            const double s = bsum[e >> 1];
+            if (e & 1) og += -fmin(s, 0.0) * dt;
+            else og += fmax(s, 0.0) * dt;
+        }
+    }
+    return og;
 }
 
 __global__ void __launch_bounds__(kBlock) ka_limit(const Ctx c, double* X, double dt)
@@ -310,14 +861,7 @@ __global__ void __launch_bounds__(kBlock) ka_limit(const Ctx c, double* X, doubl
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
     const long N = c.N;
-    const double qr = X[F_QR * N + i], qf = X[F_QF * N + i];
-    const double pos = fmax(qr, 0.0) + fmax(qf, 0.0);
-    double og = pos * dt;
-    const int c0 = c.up[i], c1 = up_end(c, i);
-    for (int u = c0; u < c1; ++u) {
-        const double neg = fmin(X[F_QR * N + u], 0.0) + fmin(X[F_QF * N + u], 0.0);
-        og += -neg * dt;
-    }
+    const double og = outgoing(c, X, i, dt);
     const double store = X[F_RS * N + i] + X[F_FS * N + i];
     X[F_LR * N + i] = (og > 1e-8) ? fmin(store / og, 1.0) : 1.0;
 }
@@ -325,20 +869,57 @@ __global__ void __launch_bounds__(kBlock) ka_limit(const Ctx c, double* X, doubl
 __global__ void __launch_bounds__(kBlock) ka_stage(const Ctx c, const double* X, double* Y,
                                                    const double* runoff, double dt)
 {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.N) return;
     const long N = c.N;
+    if ((int)blockIdx.x >= c.grid_cells) {
+        const long p = (long)(blockIdx.x - c.grid_cells) * blockDim.x + threadIdx.x;
+        if (p >= c.P) return;
+        const double lr_c = X[F_LR * N + c.bci[p]], lr_d = X[F_LR * N + c.bdi[p]];
+        const double* lim = pth(c, X, PF_BLIM);
+        double* out = pth(c, Y, PF_BOUT);
+        for (int lv = 0; lv < c.L; ++lv) {
+            const double o = lim[p * c.L + lv];
+            out[p * c.L + lv] = (o >= 0.0) ? o * lr_c : o * lr_d;
+        }
+        return;
+    }
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const uint8_t fl = c.flags[i];
     Store t;
     gather_inflow(c, X, i, t);
-    const double tot = store_eval(X[F_RS * N + i], X[F_FS * N + i], runoff[i], dt, t);
+    const double tot = store_eval(X[F_RS * N + i], X[F_FS * N + i], X[F_PS * N + i], runoff[i], dt, t);
     Stage s;
     stage_eval(c, i, tot, c.rh[i], c.rw[i], c.rl[i], s);
+    // levee cells are re-partitioned afterwards by ka_levee
     Y[F_RS * N + i] = s.rs;
     Y[F_FS * N + i] = s.fs;
-    Y[F_ROUT * N + i] = t.ur;
-    Y[F_FOUT * N + i] = t.uf;
+    Y[F_PS * N + i] = 0.0;
     Y[F_RDEP * N + i] = s.rdep;
     Y[F_FDEP * N + i] = s.fdep;
+    Y[F_PDEP * N + i] = s.fdep;
+    Y[F_ROUT * N + i] = t.ur;
+    Y[F_FOUT * N + i] = t.uf;
+    Y[F_RTI * N + i] = (c.res && (fl & CMF_CELL_RESERVOIR)) ? t.rti : 0.0;
+}
+
+// Levee re-partition of the levee cells (levee.cu:29-261) on the flood-stage
+// result ka_stage left in Y, over the compact levee list.
+__global__ void __launch_bounds__(kBlock) ka_levee(const Ctx c, double* Y)
+{
+    const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= c.NLV) return;
+    const long N = c.N;
+    const long i = c.lci[l];
+    const double in[6] = {Y[F_RS * N + i], Y[F_FS * N + i], Y[F_RDEP * N + i], Y[F_FDEP * N + i],
+                          c.rw[i], c.rh[i]};
+    double out[6], ffr = 0.0;
+    levee_part<double>(c, i, in, ffr, out);
+    Y[F_RS * N + i] = out[0];
+    Y[F_FS * N + i] = out[1];
+    Y[F_PS * N + i] = out[2];
+    Y[F_RDEP * N + i] = out[3];
+    Y[F_FDEP * N + i] = out[4];
+    Y[F_PDEP * N + i] = out[5];
 }
 
 __global__ void __launch_bounds__(kBlock) ka_cfl(const Ctx c, const double* X, double outer,
@@ -346,7 +927,7 @@ __global__ void __launch_bounds__(kBlock) ka_cfl(const Ctx c, const double* X, d
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int n_steps = 1;
-    if (i < c.N) {
+    if (i < c.N && !(c.res && (c.flags[i] & CMF_CELL_DAM_RELATED))) {
         const double dist = c.dnd[i];
         const double depth = fmax(X[F_RDEP * c.N + i], 0.01);
         double dt = c.alpha * dist / sqrt(c.g * depth);
@@ -362,13 +943,110 @@ __global__ void __launch_bounds__(kBlock) ka_cfl(const Ctx c, const double* X, d
 // reverse kernels
 // ---------------------------------------------------------------------------
 struct Adj {
-    double* lam;      // [kStateFields][N], lambda_{k+1} on entry of a sub-step, lambda_k on exit
+    double* lam;      // adjoint of a state (cell fields, then path fields)
     double* grad;     // [kGradFields][N]
     double* groff;    // [N] runoff gradient of the current interval
-    double* scr;      // [kScratchFields][N]
+    double* scr;      // cell scratch [kCellScratch][N], then path scratch
 };
 
-// Stage and storage update reversed (kr_stage).
+__device__ __forceinline__ double* lam_path(const Ctx& c, double* lam, int f)
+{
+    return lam + (long)kCellState * c.N + (long)f * c.P * c.L;
+}
+__device__ __forceinline__ double* pscr(const Ctx& c, double* scr) { return scr + (long)kCellScratch * c.N; }
+// path scratch: LRCB [P], LRDB [P], BLIMB [P*L], BCSDB [P*L], PEB [8P];
+// levee scratch: LEVB [6*NLV], LEVIN [10*NLV]
+__device__ __forceinline__ double* lrcb(const Ctx& c, double* scr) { return pscr(c, scr); }
+__device__ __forceinline__ double* lrdb(const Ctx& c, double* scr) { return pscr(c, scr) + c.P; }
+__device__ __forceinline__ double* blimb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P; }
+__device__ __forceinline__ double* bcsdb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P + c.P * c.L; }
+__device__ __forceinline__ double* peb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P + 2 * c.P * c.L; }
+__device__ __forceinline__ double* levb(const Ctx& c, double* scr) { return peb(c, scr) + 8 * c.P; }
+__device__ __forceinline__ double* levin(const Ctx& c, double* scr) { return levb(c, scr) + 6 * c.NLV; }
+
+// Apply the adjoints the later sub-step's momentum (downstream depth) and path
+// kernels (end states) left for cell i; returns nothing, updates lam / grad.
+__device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a)
+{
+    const long N = c.N;
+    double* lam = a.lam;
+    double wsum = 0.0;
+    const int c0 = c.up[i], c1 = up_end(c, i);
+    for (int u = c0; u < c1; ++u) wsum += a.scr[S_WDNB * N + u];
+    double rdep_bar = wsum, pdep_bar = 0.0, tot_bar = 0.0;
+    const uint8_t fl = c.flags[i];
+    if (c.bif && (fl & CMF_CELL_BIFURCATION)) {
+        const double* pe = peb(c, a.scr);
+        for (int b = c.bptr[i]; b < c.bptr[i + 1]; ++b) {
+            const int e = c.bpaths[b];
+            const double* q = pe + 8L * (e >> 1) + ((e & 1) ? 4 : 0);
+            rdep_bar += q[0] + q[1];
+            pdep_bar += q[2];
+            tot_bar += q[3];
+        }
+    }
+    lam[F_RDEP * N + i] += rdep_bar;
+    a.grad[G_RH * N + i] -= rdep_bar;
+    if (pdep_bar != 0.0) lam[F_PDEP * N + i] += pdep_bar;
+    if (tot_bar != 0.0) {
+        lam[F_RS * N + i] += tot_bar;
+        lam[F_FS * N + i] += tot_bar;
+        if (!(c.res && (fl & CMF_CELL_RESERVOIR))) lam[F_PS * N + i] += tot_bar;
+    }
+}
+
+// Levee re-partition reversed, over the levee list, before kr_stage.
+// kr_levee_prep completes lambda_{k+1} of the levee cell and recomputes its
+// flood stage; kr_levee runs one dual pass per levee and input direction and
+// leaves the adjoints of the flood-stage outputs (and of river width/height)
+// for kr_stage.  Compact kernels keep the long dual passes out of the
+// per-cell stage kernel.
+__global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const double* X,
+                                                        const double* runoff, double dt, Adj a)
+{
+    const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= c.NLV) return;
+    const long N = c.N;
+    const long i = c.lci[l];
+    apply_pending(c, i, a);
+    const double* lam = a.lam;
+    Store t;
+    gather_inflow(c, X, i, t);
+    const double tot = store_eval(X[F_RS * N + i], X[F_FS * N + i], X[F_PS * N + i], runoff[i], dt, t);
+    Stage s;
+    stage_eval(c, i, tot, c.rh[i], c.rw[i], c.rl[i], s);
+    double* q = levin(c, a.scr) + 10 * l;
+    q[0] = s.rs;
+    q[1] = s.fs;
+    q[2] = s.rdep;
+    q[3] = s.fdep;
+    q[4] = lam[F_RS * N + i];
+    q[5] = lam[F_FS * N + i];
+    q[6] = lam[F_PS * N + i];
+    q[7] = lam[F_RDEP * N + i];
+    q[8] = lam[F_FDEP * N + i];
+    q[9] = lam[F_PDEP * N + i];
+}
+
+__global__ void __launch_bounds__(kBlock) kr_levee(const Ctx c, Adj a)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.NLV * 6L) return;
+    const long l = t / 6;
+    const int j = (int)(t - l * 6);
+    const long i = c.lci[l];
+    const double* q = levin(c, a.scr) + 10 * l;
+    const double in[6] = {q[0], q[1], q[2], q[3], c.rw[i], c.rh[i]};
+    Dual x[6], y[6];
+    for (int k = 0; k < 6; ++k) x[k] = {in[k], k == j ? 1.0 : 0.0};
+    double ffr = 0.0;
+    levee_part<Dual>(c, i, x, ffr, y);
+    double v = 0.0;
+    for (int o = 0; o < 6; ++o) v += q[4 + o] * y[o].d;
+    levb(c, a.scr)[6 * l + j] = v;
+}
+
+// Stage, levee and storage update reversed (kr_stage).
 __global__ void __launch_bounds__(kBlock) kr_stage(const Ctx c, const double* X,
                                                    const double* runoff, double dt, Adj a)
 {
@@ -378,70 +1056,43 @@ __global__ void __launch_bounds__(kBlock) kr_stage(const Ctx c, const double* X,
     double* lam = a.lam;
     double* scr = a.scr;
     const double rw = c.rw[i], rl = c.rl[i], rh = c.rh[i];
+    const uint8_t fl = c.flags[i];
+    const bool lev_cell = c.lev && (fl & CMF_CELL_LEVEE);
+    const bool res_cell = c.res && (fl & CMF_CELL_RESERVOIR);
 
-    // lambda_{k+1} of the river depth: own part plus the pending downstream-
-    // depth adjoints of the upstream cells (their momentum read this depth).
-    double wsum = 0.0;
-    const int c0 = c.up[i], c1 = up_end(c, i);
-    for (int u = c0; u < c1; ++u) wsum += scr[S_WDNB * N + u];
-    const double L_rdep = lam[F_RDEP * N + i] + wsum;
-    double g_rh = -wsum, g_rw = 0.0;
-
-    const double L_rs = lam[F_RS * N + i], L_fs = lam[F_FS * N + i];
+    if (!lev_cell) apply_pending(c, i, a);   // levee cells: done by kr_levee
+    double L_rs = lam[F_RS * N + i], L_fs = lam[F_FS * N + i];
     const double L_rout = lam[F_ROUT * N + i], L_fout = lam[F_FOUT * N + i];
-    const double L_fdep = lam[F_FDEP * N + i];
+    double L_rdep = lam[F_RDEP * N + i], L_fdep = lam[F_FDEP * N + i];
+    const double L_pdep = lam[F_PDEP * N + i];   // protected storage' is 0 off levees
+    const double L_rti = lam[F_RTI * N + i];
+    double g_rh = 0.0, g_rw = 0.0;
 
     Store t;
     gather_inflow(c, X, i, t);
-    const double rsto = X[F_RS * N + i], fsto = X[F_FS * N + i];
-    const double tot = store_eval(rsto, fsto, runoff[i], dt, t);
+    const double rsto = X[F_RS * N + i], fsto = X[F_FS * N + i], prot = X[F_PS * N + i];
+    const double tot = store_eval(rsto, fsto, prot, runoff[i], dt, t);
     Stage s;
     stage_eval(c, i, tot, rh, rw, rl, s);
 
-    // ---- flood stage reverse -> tot_bar, rw, rh
-    double tot_bar = 0.0;
-    const double rlrw = rl * rw;
-    double rs_out_bar = L_rs + L_rdep / rlrw;       // rs' and rdep' = rs' / (rl rw)
-    g_rw += -L_rdep * s.rdep / rw;
-    if (!s.flooded) {
-        tot_bar = rs_out_bar;
+    // ---- levee re-partition reverse (outputs -> flood-stage outputs), from kr_levee
+    if (lev_cell) {
+        const double* ib = levb(c, scr) + 6L * c.lslot[i];
+        L_rs = ib[0];
+        L_fs = ib[1];
+        L_rdep = ib[2];
+        L_fdep = ib[3];
+        g_rw += ib[4];
+        g_rh += ib[5];
     } else {
-        double river_bar = rs_out_bar;
-        const double d = tot - s.rs;
-        if (!(d < 0.0)) {            // flood' = d where d >= 0
-            tot_bar += L_fs;
-            river_bar -= L_fs;
-        }
-        double cap_bar = 0.0;
-        if (s.cap_taken) cap_bar = river_bar;
-        else tot_bar += river_bar;
-        double rmax_bar = cap_bar;
-        g_rw += cap_bar * rl * s.fdep;
-        const double fdep_bar = L_fdep + cap_bar * rlrw;
-        double excess_bar, W_bar;
-        if (s.top) {
-            const double wr = s.W_tot * rl;
-            excess_bar = fdep_bar / wr;
-            W_bar = -fdep_bar * s.excess / (s.W_tot * wr);
-        } else {
-            const double dw_bar = fdep_bar * s.grad;
-            const double arg_bar = dw_bar / (2.0 * s.sq);
-            W_bar = arg_bar * 2.0 * s.W_tot - dw_bar;
-            excess_bar = arg_bar * 2.0 / (s.grad * rl);
-        }
-        tot_bar += excess_bar;
-        const double Sp_bar = -excess_bar;
-        g_rw += W_bar;
-        // S_prev = rmax + sum_{l < level} rl (W_{l-1} + W_l)/2 (H_l - H_{l-1});
-        // d/d rw of the layer sum telescopes to rl * H_{level-1}
-        rmax_bar += Sp_bar;
-        if (s.level > 0) g_rw += Sp_bar * rl * s.D_prev;
-        g_rw += rmax_bar * rl * rh;
-        g_rh += rmax_bar * rlrw;
+        L_fdep += L_pdep;   // protected depth = flood depth outside levees
     }
 
+    // ---- flood stage reverse
+    const double tot_bar = stage_reverse(s, tot, rw, rh, rl, L_rs, L_fs, L_rdep, L_fdep, g_rw, g_rh);
+
     // ---- storage update reverse
-    double tn_bar = t.total_next > 0.0 ? tot_bar : 0.0;
+    const double tn_bar = t.total_next > 0.0 ? tot_bar : 0.0;
     const double rsu3_bar = tn_bar, fsu2_bar = tn_bar;
     a.groff[i] += tn_bar * dt;
     double fsu1_bar = t.fsu1 > 0.0 ? fsu2_bar : 0.0;
@@ -455,41 +1106,91 @@ __global__ void __launch_bounds__(kBlock) kr_stage(const Ctx c, const double* X,
         rsu2_bar += rsu3_bar;
     }
     double rsu1_bar = t.rsu1 > 0.0 ? rsu2_bar : 0.0;
-    const double fs_bar = fsu1_bar;
     if (t.rsu1 < 0.0) rsu1_bar += fsu1_bar;
-    const double fin_bar = fsu1_bar * dt;
-    const double uf_own = -fsu1_bar * dt;
-    const double rs_bar = rsu1_bar;
-    const double rin_bar = rsu1_bar * dt;
-    const double ur_own = -rsu1_bar * dt;
 
-    lam[F_RS * N + i] = rs_bar;
-    lam[F_FS * N + i] = fs_bar;
-    scr[S_RINB * N + i] = rin_bar;
-    scr[S_FINB * N + i] = fin_bar;
-    scr[S_ROB * N + i] = L_rout + ur_own;
-    scr[S_FOB * N + i] = L_fout + uf_own;
+    lam[F_RS * N + i] = rsu1_bar;
+    lam[F_FS * N + i] = fsu1_bar;
+    lam[F_PS * N + i] = tn_bar;
+    lam[F_PDEP * N + i] = 0.0;
+    lam[F_RTI * N + i] = 0.0;
+    scr[S_RINB * N + i] = rsu1_bar * dt;
+    scr[S_FINB * N + i] = fsu1_bar * dt;
+    scr[S_ROB * N + i] = L_rout - rsu1_bar * dt;
+    scr[S_FOB * N + i] = L_fout - fsu1_bar * dt;
+    scr[S_GBB * N + i] = -fsu1_bar * dt;
+    scr[S_RTIB * N + i] = res_cell ? L_rti : 0.0;
     a.grad[G_RH * N + i] += g_rh;
     a.grad[G_RW * N + i] += g_rw;
 }
 
+// Path inflow reversed (kr_stage_path): net flux into the end cells and the
+// limit-rate scaling of the level fluxes.
+__global__ void __launch_bounds__(kBlock) kr_stage_path(const Ctx c, const double* X, Adj a)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= c.P) return;
+    const long N = c.N;
+    const int L = c.L;
+    const int ci = c.bci[p], di = c.bdi[p];
+    const double lr_c = X[F_LR * N + ci], lr_d = X[F_LR * N + di];
+    const double raw = braw_of(c, X)[p];
+    const double net_bar = a.scr[S_GBB * N + ci] - a.scr[S_GBB * N + di];
+    double lrc_bar = 0.0, lrd_bar = 0.0;
+    double raw_bar;
+    if (raw >= 0.0) {
+        raw_bar = net_bar * lr_c;
+        lrc_bar += net_bar * raw;
+    } else {
+        raw_bar = net_bar * lr_d;
+        lrd_bar += net_bar * raw;
+    }
+    const double* lim = pth(c, X, PF_BLIM);
+    double* lb = lam_path(c, a.lam, PF_BOUT);
+    double* bb = blimb(c, a.scr);
+    for (int lv = 0; lv < L; ++lv) {
+        const double o = lim[p * L + lv];
+        const double lam_o = lb[p * L + lv];
+        double ob = raw_bar;
+        if (o >= 0.0) {
+            ob += lam_o * lr_c;
+            lrc_bar += lam_o * o;
+        } else {
+            ob += lam_o * lr_d;
+            lrd_bar += lam_o * o;
+        }
+        bb[p * L + lv] = ob;
+    }
+    lrcb(c, a.scr)[p] = lrc_bar;
+    lrdb(c, a.scr)[p] = lrd_bar;
+    // lambda_{k+1} of the path cross-section depths, read by every direction
+    // thread of kr_path while some of them write lambda_k in place
+    const double* lc = lam_path(c, a.lam, PF_BCSD);
+    double* cb = bcsdb(c, a.scr);
+    for (int lv = 0; lv < L; ++lv) cb[p * L + lv] = lc[p * L + lv];
+}
+
 // Limit-rate adjoint (kr_limit).  u_j = q_j * (q_j >= 0 ? lr_j : lr_dn(j))
-// enters the cell's own update (-u dt) and its downstream inflow (+u dt), so
-// its adjoint is rob_j + rinb_dn(j); lr_j collects the positive own fluxes and
-// the negative fluxes of the upstream cells.
+// enters the cell's own update (-u dt), its downstream inflow (+u dt) and, for
+// a reservoir downstream, that reservoir's inflow record; lr_j collects the
+// positive own fluxes, the negative fluxes of the upstream cells and the path
+// terms of its bifurcation ends.
 __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X, double dt, Adj a)
 {
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= c.N) return;
     const long N = c.N;
     const double* scr = a.scr;
-    const bool mouth = c.flags[j] & CMF_CELL_MOUTH;
+    const uint8_t fl = c.flags[j];
+    const bool mouth = fl & CMF_CELL_MOUTH;
     const int dn = c.dn[j];
     const double qr = X[F_QR * N + j], qf = X[F_QF * N + j], lr = X[F_LR * N + j];
     const double lr_dn = mouth ? lr : X[F_LR * N + dn];
     const double rinb = scr[S_RINB * N + j], finb = scr[S_FINB * N + j];
-    const double a_r = scr[S_ROB * N + j] + (mouth ? 0.0 : scr[S_RINB * N + dn]);
-    const double a_f = scr[S_FOB * N + j] + (mouth ? 0.0 : scr[S_FINB * N + dn]);
+    const double rtib = scr[S_RTIB * N + j];
+    const double dn_r = mouth ? 0.0 : scr[S_RINB * N + dn] + scr[S_RTIB * N + dn];
+    const double dn_f = mouth ? 0.0 : scr[S_FINB * N + dn] + scr[S_RTIB * N + dn];
+    const double a_r = scr[S_ROB * N + j] + dn_r;
+    const double a_f = scr[S_FOB * N + j] + dn_f;
 
     double lr_bar = 0.0;
     if (qr >= 0.0 || mouth) lr_bar += a_r * qr;
@@ -501,9 +1202,21 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
     const int c0 = c.up[j], c1 = up_end(c, j);
     for (int u = c0; u < c1; ++u) {
         const double cr = X[F_QR * N + u], cf = X[F_QF * N + u];
-        if (cr < 0.0) lr_bar += (scr[S_ROB * N + u] + rinb) * cr;
-        if (cf < 0.0) lr_bar += (scr[S_FOB * N + u] + finb) * cf;
+        if (cr < 0.0) lr_bar += (scr[S_ROB * N + u] + rinb + rtib) * cr;
+        if (cf < 0.0) lr_bar += (scr[S_FOB * N + u] + finb + rtib) * cf;
         og += -(fmin(cr, 0.0) + fmin(cf, 0.0)) * dt;
+    }
+    if (c.bif && (fl & CMF_CELL_BIFURCATION)) {
+        const double* bsum = bsum_of(c, X);
+        double* ps_ = a.scr + (long)kCellScratch * N;
+        for (int b = c.bptr[j]; b < c.bptr[j + 1]; ++b) {
+            const int e = c.bpaths[b];
+            const int p = e >> 1;
+            lr_bar += (e & 1) ? ps_[c.P + p] : ps_[p];
+            const double s = bsum[p];
+            if (e & 1) og += -fmin(s, 0.0) * dt;
+            else og += fmax(s, 0.0) * dt;
+        }
     }
 
     double og_bar = 0.0;
@@ -524,34 +1237,96 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
     a.scr[S_QFB * N + j] = qf_bar;
 }
 
-// Momentum reversed (kr_momentum): lambda_k of the cell, the downstream-depth
-// adjoint left for the downstream cell's next kr_stage, parameter gradients.
-__global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double* X, double dt, Adj a)
+// Path momentum reversed (kr_path): one thread per path and input direction
+// (6 end-state inputs and two per level) evaluates one dual pass of the path
+// flux and writes that input's adjoint: lambda_k of the path state, or an
+// end-state adjoint left for the end cell.
+__global__ void __launch_bounds__(kBlock) kr_path(const Ctx c, const double* X, double dt, Adj a)
 {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.N) return;
+    const int L = c.L;
+    const int NI = 6 + 2 * L;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.P * (long)NI) return;
+    const long p = t / NI;
+    const int j = (int)(t - p * NI);
+    const long N = c.N;
+    const int ci = c.bci[p], di = c.bdi[p];
+    double in[6 + 2 * kMaxLevels];
+    path_inputs(c, X, p, in);
+    Dual x[6 + 2 * kMaxLevels];
+    for (int q = 0; q < NI; ++q) x[q] = {in[q], q == j ? 1.0 : 0.0};
+    Dual blim[kMaxLevels], bcsd_new[kMaxLevels], bs;
+    path_flux<Dual>(c, p, x, dt, blim, bs, bcsd_new);
+    const double bsum = bsum_of(c, X)[p];
+    double sb = 0.0;
+    if (bsum >= 0.0) sb += a.scr[S_OGB * N + ci] * dt;
+    if (bsum <= 0.0) sb -= a.scr[S_OGB * N + di] * dt;
+    const double* bb = blimb(c, a.scr);
+    const double* cb = bcsdb(c, a.scr);
+    double v = sb * bs.d;
+    for (int lv = 0; lv < L; ++lv) v += bb[p * L + lv] * blim[lv].d + cb[p * L + lv] * bcsd_new[lv].d;
+    if (j >= 6 + L) {
+        lam_path(c, a.lam, PF_BCSD)[p * L + (j - 6 - L)] = v;
+    } else if (j >= 6) {
+        lam_path(c, a.lam, PF_BOUT)[p * L + (j - 6)] = v;
+    } else {
+        // end state: [wse, protected-WSE part on the WSE, protected depth, total storage]
+        const int end = j & 1;
+        double* q = peb(c, a.scr) + 8L * p + 4 * end;
+        if (j < 2) {
+            q[0] = v;
+        } else if (j < 4) {
+            const int e = end ? di : ci;
+            bool to_pdep = false;
+            if (c.lev && (c.flags[e] & CMF_CELL_LEVEE)) {
+                const double wse = X[F_RDEP * N + e] + (c.celv[e] - c.rh[e]);
+                to_pdep = c.celv[e] + X[F_PDEP * N + e] <= wse;
+            }
+            q[1] = to_pdep ? 0.0 : v;
+            q[2] = to_pdep ? v : 0.0;
+        } else {
+            q[3] = v;
+        }
+    }
+}
+
+// Momentum reversed (kr_momentum): lambda_k of the cell, the downstream-depth
+// adjoint left for the downstream cell, parameter gradients.
+__global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double* X,
+                                                      const double* runoff, double dt, Adj a)
+{
     const long N = c.N;
     double* lam = a.lam;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
     Mom m;
     mom_eval(c, X, i, dt, m);
-    const double D = c.g * dt;
+    const double Dg = c.g * dt;
+    const uint8_t fl = c.flags[i];
 
-    // adjoints of the final fluxes: stage/limiter part, plus the outgoing
-    // storage of the downstream cell (negative fluxes leave through it)
     double qr_bar = a.scr[S_QRB * N + i];
     double qf_bar = a.scr[S_QFB * N + i];
+    double qr_final, qf_final;
+    cell_flux(c, X, runoff, i, dt, m, qr_final, qf_final);
     if (!m.mouth) {
         const double ogb_dn = a.scr[S_OGB * N + m.dn];
-        if (m.qr <= 0.0) qr_bar += -ogb_dn * dt;
-        if (m.qf <= 0.0) qf_bar += -ogb_dn * dt;
+        if (qr_final <= 0.0) qr_bar += -ogb_dn * dt;
+        if (qf_final <= 0.0) qf_bar += -ogb_dn * dt;
     }
     double ucsd_bar = lam[F_RCSD * N + i];
     double ufcsd_bar = lam[F_FCSD * N + i];
     double ufcsa_bar = lam[F_FCSA * N + i];
 
-    double rs_bar = 0.0, fs_bar = 0.0, rout_bar = 0.0, fout_bar = 0.0, rdep_bar = 0.0;
+    double rs_bar = 0.0, fs_bar = 0.0, ps_bar = 0.0, rout_bar = 0.0, fout_bar = 0.0, rdep_bar = 0.0;
     double fdep_bar = 0.0, rcsd_bar = 0.0, fcsd_bar = 0.0, fcsa_bar = 0.0;
     double g_rman = 0.0, g_fman = 0.0, g_rw = 0.0, relev_bar = 0.0;
+
+    // the dam-upstream kinematic flow and the reservoir release replace the
+    // flux of those cells; kr_dam reverses them
+    if (c.res && (fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) {
+        qr_bar = 0.0;
+        qf_bar = 0.0;
+    }
 
     // negative-flow limiter
     double qr0_bar = qr_bar, qf1_bar = qf_bar;
@@ -564,6 +1339,7 @@ __global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double*
             const double tnf_bar = -lrn_bar * m.lrn_raw / m.tnf;
             rs_bar += tsf_bar;
             fs_bar += tsf_bar;
+            ps_bar += tsf_bar;
             qr0_bar += -tnf_bar * dt;
             qf1_bar += -tnf_bar * dt;
         }
@@ -571,20 +1347,19 @@ __global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double*
     const double qf0_bar = m.zero_f ? 0.0 : qf1_bar;
 
     double slope_bar = 0.0, fslope_bar = 0.0, r_sifd_bar = 0.0, f_sifd_bar = 0.0;
-    // floodplain flux
     if (m.fc) {
         const double numf_bar = qf0_bar / m.denf;
         const double denf_bar = -qf0_bar * m.qf0_val / m.denf;
         fout_bar += numf_bar;
-        double fimp_bar = numf_bar * D * fmin(fmax(m.slope, -0.005), 0.005);
-        fslope_bar += numf_bar * D * m.fimp;
+        double fimp_bar = numf_bar * Dg * fmin(fmax(m.slope, -0.005), 0.005);
+        fslope_bar += numf_bar * Dg * m.fimp;
         const double af = fabs(m.fout);
         const double B = 1.0 / (m.f_sifd * cbrt(m.f_sifd));
         const double nf2 = m.fman * m.fman;
-        const double T = D * nf2 * af * B / m.fimp;
-        g_fman += denf_bar * D * 2.0 * m.fman * af * B / m.fimp;
-        fout_bar += denf_bar * D * nf2 * B / m.fimp * sgn(m.fout);
-        f_sifd_bar += denf_bar * D * nf2 * af / m.fimp * (-(4.0 / 3.0) * B / m.f_sifd);
+        const double T = Dg * nf2 * af * B / m.fimp;
+        g_fman += denf_bar * Dg * 2.0 * m.fman * af * B / m.fimp;
+        fout_bar += denf_bar * Dg * nf2 * B / m.fimp * sgn(m.fout);
+        f_sifd_bar += denf_bar * Dg * nf2 * af / m.fimp * (-(4.0 / 3.0) * B / m.f_sifd);
         fimp_bar += denf_bar * (-T / m.fimp);
         if (m.P3 > kFloor2) {
             const double P3_bar = fimp_bar / (2.0 * m.s3);
@@ -592,39 +1367,35 @@ __global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double*
             if (m.fcsa >= kFloor) fcsa_bar += P3_bar * m.ufcsa;
         }
     }
-    // river flux
     if (m.rc) {
         const double num_bar = qr0_bar / m.den;
         const double den_bar = -qr0_bar * m.qr0_val / m.den;
-        g_rw += num_bar * (m.q + D * m.r_sifd * m.slope);
+        g_rw += num_bar * (m.q + Dg * m.r_sifd * m.slope);
         const double inner_bar = num_bar * m.rw;
         double q_bar = inner_bar;
-        r_sifd_bar += inner_bar * D * m.slope;
-        slope_bar += inner_bar * D * m.r_sifd;
+        r_sifd_bar += inner_bar * Dg * m.slope;
+        slope_bar += inner_bar * Dg * m.r_sifd;
         const double aq = fabs(m.q);
         const double Br = 1.0 / (m.r_sifd * m.r_sifd * cbrt(m.r_sifd));
         const double n2 = m.rman * m.rman;
-        g_rman += den_bar * D * 2.0 * m.rman * aq * Br;
-        q_bar += den_bar * D * n2 * Br * sgn(m.q);
-        r_sifd_bar += den_bar * D * n2 * aq * (-(7.0 / 3.0) * Br / m.r_sifd);
+        g_rman += den_bar * Dg * 2.0 * m.rman * aq * Br;
+        q_bar += den_bar * Dg * n2 * Br * sgn(m.q);
+        r_sifd_bar += den_bar * Dg * n2 * aq * (-(7.0 / 3.0) * Br / m.r_sifd);
         rout_bar += q_bar / m.rw;
         g_rw += -q_bar * m.q / m.rw;
     }
     if (m.slope >= -0.005 && m.slope <= 0.005) slope_bar += fslope_bar;
-    // flood cross-section area
     if (m.ufcsa_raw >= 0.0) {
         fs_bar += ufcsa_bar / m.rl;
         fdep_bar += -ufcsa_bar * m.rw;
         g_rw += -ufcsa_bar * m.fdep;
     }
-    // flood cross-section depth
     if (m.P2 > kFloor2) {
         const double P2_bar = f_sifd_bar / (2.0 * m.s2);
         ufcsd_bar += P2_bar * m.fcsd;
         fcsd_bar += P2_bar * m.ufcsd;
     }
     double fsurf_bar = (m.fsurf_m >= 0.0) ? ufcsd_bar : 0.0;
-    // river cross-section depth
     if (m.P1 > kFloor2) {
         const double P1_bar = r_sifd_bar / (2.0 * m.s1);
         ucsd_bar += P1_bar * m.rcsd;
@@ -649,6 +1420,7 @@ __global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double*
 
     lam[F_RS * N + i] += rs_bar;
     lam[F_FS * N + i] += fs_bar;
+    lam[F_PS * N + i] += ps_bar;
     lam[F_ROUT * N + i] = rout_bar;
     lam[F_FOUT * N + i] = fout_bar;
     lam[F_RDEP * N + i] = rdep_bar;
@@ -663,17 +1435,71 @@ __global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double*
     a.grad[G_RW * N + i] += g_rw;
 }
 
-// Apply the pending downstream-depth adjoints (end of the reverse sweep).
+// Flux adjoints of a cell after kr_limit: the stage/limiter part plus the
+// outgoing storage of its downstream cell.
+__device__ __forceinline__ void flux_bars(const Ctx& c, const double* X, const Adj& a, long i,
+                                          double dt, double& qr_bar, double& qf_bar)
+{
+    const long N = c.N;
+    qr_bar = a.scr[S_QRB * N + i];
+    qf_bar = a.scr[S_QFB * N + i];
+    if (!(c.flags[i] & CMF_CELL_MOUTH)) {
+        const double ogb_dn = a.scr[S_OGB * N + c.dn[i]];
+        if (X[F_QR * N + i] <= 0.0) qr_bar += -ogb_dn * dt;
+        if (X[F_QF * N + i] <= 0.0) qf_bar += -ogb_dn * dt;
+    }
+}
+
+// Reservoir release and dam-upstream kinematic flow reversed (kr_dam), one
+// thread per cell (the others return at once), after kr_momentum: it adds to
+// what kr_momentum wrote.
+__global__ void __launch_bounds__(kBlock) kr_dam(const Ctx c, const double* X,
+                                                 const double* runoff, double dt, Adj a)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const uint8_t fl = c.flags[i];
+    if (!(fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) return;
+    const long N = c.N;
+    double* lam = a.lam;
+    double qr_bar, qf_bar;
+    flux_bars(c, X, a, i, dt, qr_bar, qf_bar);
+    if (fl & CMF_CELL_RESERVOIR) {
+        const double in[4] = {X[F_RS * N + i], X[F_FS * N + i], X[F_RTI * N + i], runoff[i]};
+        const double ob[1] = {qr_bar};
+        double ib[4] = {0, 0, 0, 0};
+        const int slot = c.rslot[i];
+        vjp<4, 1>(in, ob, ib, [&](const Dual* x, Dual* y) {
+            y[0] = release<Dual>(c, slot, x[0], x[1], x[2], x[3], dt);
+        });
+        lam[F_RS * N + i] += ib[0];
+        lam[F_FS * N + i] += ib[1];
+        lam[F_RTI * N + i] += ib[2];
+        a.groff[i] += ib[3];
+    } else {
+        const double in[7] = {X[F_RDEP * N + i], X[F_FDEP * N + i], X[F_RS * N + i],
+                              X[F_FS * N + i], c.rw[i], c.rman[i], c.fman[i]};
+        const double ob[2] = {qr_bar, qf_bar};
+        double ib[7] = {0, 0, 0, 0, 0, 0, 0};
+        vjp<7, 2>(in, ob, ib, [&](const Dual* x, Dual* y) {
+            kinematic<Dual>(c, i, x[0], x[1], x[2], x[3], x[4], x[5], x[6], dt, y[0], y[1]);
+        });
+        lam[F_RDEP * N + i] += ib[0];
+        lam[F_FDEP * N + i] += ib[1];
+        lam[F_RS * N + i] += ib[2];
+        lam[F_FS * N + i] += ib[3];
+        a.grad[G_RW * N + i] += ib[4];
+        a.grad[G_RMAN * N + i] += ib[5];
+        a.grad[G_FMAN * N + i] += ib[6];
+    }
+}
+
+// Apply the pending adjoints of the last reversed sub-step (end of the sweep).
 __global__ void __launch_bounds__(kBlock) kr_finalize(const Ctx c, Adj a)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
-    const long N = c.N;
-    double wsum = 0.0;
-    const int c0 = c.up[i], c1 = up_end(c, i);
-    for (int u = c0; u < c1; ++u) wsum += a.scr[S_WDNB * N + u];
-    a.lam[F_RDEP * N + i] += wsum;
-    a.grad[G_RH * N + i] -= wsum;
+    apply_pending(c, i, a);
 }
 
 }  // namespace
@@ -690,15 +1516,23 @@ int launch_status()
     return cudaGetLastError() == cudaSuccess ? CMF_OK : CMF_ERR_CUDA;
 }
 
+long scratch_len(const Ctx& c)
+{
+    return (long)kCellScratch * c.N + 2 * c.P + 2 * c.P * c.L + 8 * c.P + 16 * c.NLV;
+}
+
 }  // namespace
 
 extern "C" {
 
-int cmf_adj_layout(int* state_fields, int* slot_fields, int* scratch_fields, int* grad_fields)
+int cmf_adj_sizes(const CmfAdjPlan* plan, int64_t* state_len, int64_t* slot_len,
+                  int64_t* scratch_doubles, int* grad_fields)
 {
-    if (state_fields) *state_fields = kStateFields;
-    if (slot_fields) *slot_fields = kSlotFields;
-    if (scratch_fields) *scratch_fields = kScratchFields;
+    if (!plan) return CMF_ERR_ARG;
+    const Ctx& c = plan->ctx;
+    if (state_len) *state_len = (int64_t)kCellState * c.N + 2 * c.P * c.L;
+    if (slot_len) *slot_len = c.slot_len;
+    if (scratch_doubles) *scratch_doubles = scratch_len(c);
     if (grad_fields) *grad_fields = kGradFields;
     return CMF_OK;
 }
@@ -709,10 +1543,9 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
     *out = nullptr;
     if (v->abi_version != CMF_ABI_VERSION) return CMF_ERR_ARG;
     if (!(v->features & CMF_FEAT_FP64)) return CMF_ERR_UNSUPPORTED;
-    if (v->features & (CMF_FEAT_BIFURCATION | CMF_FEAT_LEVEE | CMF_FEAT_RESERVOIR))
-        return CMF_ERR_UNSUPPORTED;
     if (v->num_members != 1 || v->batched_mask != 0) return CMF_ERR_UNSUPPORTED;
-    if (v->num_catchments < 1 || v->num_catchments > (1L << 31) - 2 || v->num_flood_levels < 1)
+    if (v->num_catchments < 1 || v->num_catchments > (1L << 31) - 2 || v->num_flood_levels < 1 ||
+        v->num_flood_levels > kMaxFloodLevels)
         return CMF_ERR_ARG;
     const void* need[] = {v->downstream_idx, v->upstream_ptr, v->cell_flags, v->river_width,
                           v->river_length, v->river_height, v->catchment_elevation,
@@ -720,14 +1553,36 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
                           v->flood_manning, v->flood_depth_table};
     for (const void* p : need)
         if (!p) return CMF_ERR_ARG;
+    const bool lev = v->features & CMF_FEAT_LEVEE;
+    const bool res = v->features & CMF_FEAT_RESERVOIR;
+    const bool bif = v->features & CMF_FEAT_BIFURCATION;
+    if (lev && (!v->levee_slot || !v->levee_catchment_idx || !v->levee_crown_height || !v->levee_fraction ||
+                !v->levee_base_height))
+        return CMF_ERR_ARG;
+    if (res && (!v->reservoir_slot || !v->reservoir_catchment_idx || !v->conservation_volume || !v->emergency_volume ||
+                !v->adjustment_volume || !v->effective_normal_outflow ||
+                !v->adjustment_outflow || !v->flood_control_outflow))
+        return CMF_ERR_ARG;
+    if (bif && (!v->bif_cell_ptr || !v->bif_cell_paths || !v->bifurcation_catchment_idx ||
+                !v->bifurcation_downstream_idx || !v->bifurcation_manning ||
+                !v->bifurcation_width || !v->bifurcation_length || !v->bifurcation_elevation ||
+                v->num_bifurcation_levels < 1 || v->num_bifurcation_levels > kMaxLevels))
+        return CMF_ERR_ARG;
     CmfAdjPlan* p = new (std::nothrow) CmfAdjPlan;
     if (!p) return CMF_ERR_ARG;
+    std::memset(p, 0, sizeof(CmfAdjPlan));
     Ctx& c = p->ctx;
     c.N = v->num_catchments;
     c.K = v->num_flood_levels;
+    c.lev = lev;
+    c.res = res;
+    c.bif = bif;
+    c.P = bif ? v->num_bifurcation_paths : 0;
+    c.L = bif ? v->num_bifurcation_levels : 0;
     c.g = v->gravity;
     c.alpha = v->adaptive_time_factor;
     c.max_dt = v->max_sub_step_seconds;
+    c.min_kin = v->min_kinematic_slope;
     c.dn = static_cast<const int*>(v->downstream_idx);
     c.up = static_cast<const int*>(v->upstream_ptr);
     c.flags = static_cast<const uint8_t*>(v->cell_flags);
@@ -740,7 +1595,40 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
     c.rman = static_cast<const double*>(v->river_manning);
     c.fman = static_cast<const double*>(v->flood_manning);
     c.tbl = static_cast<const double*>(v->flood_depth_table);
-    p->grid = (int)((c.N + kBlock - 1) / kBlock);
+    if (lev) {
+        c.NLV = v->num_levees;
+        c.lci = v->levee_catchment_idx;
+        c.lslot = v->levee_slot;
+        c.lcrown = static_cast<const double*>(v->levee_crown_height);
+        c.lfrac = static_cast<const double*>(v->levee_fraction);
+        c.lbase = static_cast<const double*>(v->levee_base_height);
+    }
+    if (res) {
+        c.R = v->num_reservoirs;
+        c.rci = v->reservoir_catchment_idx;
+        c.rslot = v->reservoir_slot;
+        c.rcons = static_cast<const double*>(v->conservation_volume);
+        c.remerg = static_cast<const double*>(v->emergency_volume);
+        c.radj = static_cast<const double*>(v->adjustment_volume);
+        c.rnout = static_cast<const double*>(v->effective_normal_outflow);
+        c.raout = static_cast<const double*>(v->adjustment_outflow);
+        c.rfcout = static_cast<const double*>(v->flood_control_outflow);
+    }
+    if (bif) {
+        c.bptr = v->bif_cell_ptr;
+        c.bpaths = v->bif_cell_paths;
+        c.bci = v->bifurcation_catchment_idx;
+        c.bdi = v->bifurcation_downstream_idx;
+        c.bman = static_cast<const double*>(v->bifurcation_manning);
+        c.bwid = static_cast<const double*>(v->bifurcation_width);
+        c.blen = static_cast<const double*>(v->bifurcation_length);
+        c.belv = static_cast<const double*>(v->bifurcation_elevation);
+    }
+    c.path_off = (long)kSlotCell * c.N;
+    c.slot_len = c.path_off + 3L * c.P * c.L + 2 * c.P;
+    c.grid_cells = (int)((c.N + kBlock - 1) / kBlock);
+    c.grid_paths = (int)((c.P + kBlock - 1) / kBlock);
+    p->grid = c.grid_cells;
     *out = p;
     return CMF_OK;
 }
@@ -763,13 +1651,16 @@ int cmf_adj_forward(CmfAdjPlan* plan, void* stream, double* slots, int num_sub_s
     if (!plan || !slots || !runoff || num_sub_steps < 0 || !(dt > 0.0)) return CMF_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Ctx& c = plan->ctx;
-    const long stride = (long)kSlotFields * c.N;
+    const long stride = c.slot_len;
+    const int grid_all = c.grid_cells + (c.bif ? c.grid_paths : 0);
     for (int k = 0; k < num_sub_steps; ++k) {
         double* X = slots + (keep_tape ? (long)k : (long)(k & 1)) * stride;
         double* Y = slots + (keep_tape ? (long)(k + 1) : (long)((k + 1) & 1)) * stride;
-        ka_momentum<<<plan->grid, kBlock, 0, s>>>(c, X, Y, dt);
-        ka_limit<<<plan->grid, kBlock, 0, s>>>(c, X, dt);
-        ka_stage<<<plan->grid, kBlock, 0, s>>>(c, X, Y, runoff, dt);
+        ka_momentum<<<grid_all, kBlock, 0, s>>>(c, X, Y, runoff, dt);
+        ka_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt);
+        ka_stage<<<grid_all, kBlock, 0, s>>>(c, X, Y, runoff, dt);
+        if (c.lev && c.NLV > 0)
+            ka_levee<<<(int)((c.NLV + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, Y);
     }
     return launch_status();
 }
@@ -783,13 +1674,21 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         return CMF_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Ctx& c = plan->ctx;
-    const long stride = (long)kSlotFields * c.N;
+    const long stride = c.slot_len;
     Adj a{lambda, grad_params, grad_runoff, scratch};
     for (int k = num_sub_steps - 1; k >= 0; --k) {
         const double* X = tape + (long)k * stride;
-        kr_stage<<<plan->grid, kBlock, 0, s>>>(c, X, runoff, dt, a);
-        kr_limit<<<plan->grid, kBlock, 0, s>>>(c, X, dt, a);
-        kr_momentum<<<plan->grid, kBlock, 0, s>>>(c, X, dt, a);
+        if (c.lev && c.NLV > 0) {
+            kr_levee_prep<<<(int)((c.NLV + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, runoff, dt, a);
+            kr_levee<<<(int)((c.NLV * 6 + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, a);
+        }
+        kr_stage<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        if (c.bif) kr_stage_path<<<c.grid_paths, kBlock, 0, s>>>(c, X, a);
+        kr_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt, a);
+        kr_momentum<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        if (c.res && c.R > 0) kr_dam<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        if (c.bif)
+            kr_path<<<(int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, dt, a);
     }
     return launch_status();
 }

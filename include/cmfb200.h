@@ -285,38 +285,45 @@ int cmf_substep_noalloc(const CmfView* view, void* stream, int diag);
 int cmf_budget_flush(CmfPlan* plan, void* stream);
 
 /* ---- adjoint of the sub-step (no counterpart in the reference) -----------
- * Reverse mode of the base-physics sub-step in fp64, for gradients of a loss
- * on discharge with respect to the Manning coefficients, river height, river
- * width, runoff and the initial state.  It differentiates the forward of
- * cmfgpu/phys/cuda/outflow.cu:21-222 and storage.cu:22-226 in the step order
- * of cmfgpu/models/cama_flood_model.py:134-162.
+ * Reverse mode of the routing sub-step in fp64, every physics module, for
+ * gradients of a loss on discharge with respect to the Manning coefficients,
+ * river height, river width, runoff and the initial state.  It differentiates
+ * the forward of cmfgpu/phys/cuda/outflow.cu, reservoir.cu, bifurcation.cu,
+ * storage.cu and levee.cu in the step order of
+ * cmfgpu/models/cama_flood_model.py:134-162.
  *
- * Layout (N = view.num_catchments, all doubles, field-major):
- *   state  [9][N]   river storage, flood storage, river outflow, flood outflow,
- *                   river depth, flood depth, river cross-section depth,
- *                   flood cross-section depth, flood cross-section area
- *   slot   [12][N]  a state plus the sub-step's river/flood flux and limit rate
- *   lambda [9][N]   adjoint of a state (same field order)
- *   grad   [4][N]   river Manning, flood Manning, river height, river width
- *   scratch[8][N]   reverse-sweep intermediates; zero it before a sweep
- * cmf_adj_layout reports these counts.
+ * Layout (N = catchments, P = bifurcation paths, L = levels; doubles):
+ *   state   [12][N] river storage, flood storage, river outflow, flood
+ *                   outflow, river depth, flood depth, river cross-section
+ *                   depth, flood cross-section depth, flood cross-section
+ *                   area, protected storage, protected depth, reservoir
+ *                   total inflow; then [2][P*L] bifurcation outflow and
+ *                   cross-section depth
+ *   slot    a state's cell fields plus the sub-step's river/flood flux and
+ *           limit rate ([15][N]), then the path state and the limited path
+ *           fluxes ([3][P*L] + [2][P]); its length comes from cmf_adj_sizes
+ *   lambda  adjoint of a state (state layout)
+ *   grad    [4][N] river Manning, flood Manning, river height, river width
+ *   scratch reverse-sweep intermediates; zero it before a sweep
  *
- * The view must have CMF_FEAT_FP64, one member and none of the bifurcation,
- * levee or reservoir features (else CMF_ERR_UNSUPPORTED).  The plan keeps the
- * view's topology and parameter pointers; the differentiated parameters are
- * read through river_manning, flood_manning, river_height and river_width.
- * All work is queued on `stream`; nothing is allocated. */
+ * The view must have CMF_FEAT_FP64 and one member (else
+ * CMF_ERR_UNSUPPORTED).  The plan keeps the view's topology and parameter
+ * pointers; the differentiated parameters are read through river_manning,
+ * flood_manning, river_height and river_width.  All work is queued on
+ * `stream`; nothing is allocated. */
 typedef struct CmfAdjPlan CmfAdjPlan;
-int cmf_adj_layout(int* state_fields, int* slot_fields, int* scratch_fields,
-                   int* grad_fields);
 int cmf_adj_plan_create(const CmfView* view, CmfAdjPlan** out);
 void cmf_adj_plan_destroy(CmfAdjPlan* plan);
+/* Lengths (doubles) of a state, a tape slot and the scratch, and the number
+ * of gradient fields, for this plan. */
+int cmf_adj_sizes(const CmfAdjPlan* plan, int64_t* state_len, int64_t* slot_len,
+                  int64_t* scratch_len, int* grad_fields);
 /* CFL sub-step count of the state in `slot` for one forcing interval
  * (adaptive_time.cu:19-48) into *n_device (a device int). */
 int cmf_adj_sub_steps(CmfAdjPlan* plan, void* stream, const double* slot,
                       double outer_seconds, int* n_device);
 /* num_sub_steps forward sub-steps of length dt with forcing `runoff` [N].
- * keep_tape != 0: slots[k] (k = 0..n, stride 12N) receives X_k and the
+ * keep_tape != 0: slots[k] (k = 0..n, stride slot_len) receives X_k and the
  * sub-step's fluxes; the caller fills the state of slots[0].  keep_tape == 0:
  * two slots ping-pong and the final state is in slots[n & 1]. */
 int cmf_adj_forward(CmfAdjPlan* plan, void* stream, double* slots,
@@ -330,8 +337,9 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape,
                     int num_sub_steps, const double* runoff, double dt,
                     double* lambda, double* grad_params, double* grad_runoff,
                     double* scratch);
-/* Add the pending downstream-depth terms of the last reversed sub-step to
- * lambda (river depth) and grad (river height); call once after the sweep. */
+/* Add the pending terms of the last reversed sub-step (downstream depth read
+ * by momentum, end states read by the paths) to lambda and grad (river
+ * height); call once after the sweep. */
 int cmf_adj_finalize(CmfAdjPlan* plan, void* stream, double* lambda,
                      double* grad_params, double* scratch);
 
