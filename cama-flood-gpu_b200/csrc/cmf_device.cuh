@@ -51,6 +51,7 @@ template <typename REAL>
 struct Dev {
     long N;
     int M;
+    int mshift;   // log2(M) when M is a power of two, else -1
     int K;
     long P;
     int L;
@@ -107,6 +108,24 @@ struct Dev {
 // ---------------------------------------------------------------------------
 template <bool ONE>
 __device__ __forceinline__ long ix(long i, int m, int M) { return ONE ? i : i * (long)M + m; }
+
+// (item, member) of flat thread index t over [items, M]: a shift and a mask
+// when M is a power of two, a division otherwise.
+template <bool ONE, typename REAL>
+__device__ __forceinline__ long split_member(const Dev<REAL>& v, long t, int& m)
+{
+    if (ONE) {
+        m = 0;
+        return t;
+    }
+    if (v.mshift >= 0) {
+        m = (int)(t & ((1L << v.mshift) - 1));
+        return t >> v.mshift;
+    }
+    const long i = t / v.M;
+    m = (int)(t - i * v.M);
+    return i;
+}
 
 template <bool ONE, typename REAL>
 __device__ __forceinline__ REAL par(const REAL* p, int bit, int batched, long i, int m, int M)
@@ -471,15 +490,15 @@ __global__ void __launch_bounds__(256) k_momentum(const Dev<REAL> v, int kh, int
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
         long t = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
         if (t >= v.P * (long)v.M) return;
-        long p = ONE ? t : t / v.M;
-        int m = ONE ? 0 : (int)(t - p * v.M);
+        int m;
+        long p = split_member<ONE>(v, t, m);
         momentum_path<REAL, ONE, RES, LEV>(v, p, m, kh);
         return;
     }
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= v.N * (long)v.M) return;
-    long i = ONE ? t : t / v.M;
-    int m = ONE ? 0 : (int)(t - i * v.M);
+    int m;
+    long i = split_member<ONE>(v, t, m);
     momentum_cell<REAL, ONE, RES, LEV, BIF>(v, i, m, kh, force_diag);
 }
 
@@ -1019,12 +1038,12 @@ __device__ __forceinline__ void stage_path(const Dev<REAL>& v, long p, int m, in
 // cell and its bifurcation partners.
 // ---------------------------------------------------------------------------
 template <typename REAL, bool ONE, bool BIF>
-__global__ void __launch_bounds__(256) k_limit(const Dev<REAL> v, int kh)
+__global__ void __launch_bounds__(256, (sizeof(REAL) == 4 ? 8 : 4)) k_limit(const Dev<REAL> v, int kh)
 {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= v.N * (long)v.M) return;
-    long i = ONE ? t : t / v.M;
-    int m = ONE ? 0 : (int)(t - i * v.M);
+    int m;
+    long i = split_member<ONE>(v, t, m);
     const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
     if (!st.active) return;
     const int k = st.k;
@@ -1064,8 +1083,8 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
 {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < v.NLV * (long)v.M) {
-        const long li = ONE ? t : t / v.M;
-        const int m = ONE ? 0 : (int)(t - li * v.M);
+        int m;
+        const long li = split_member<ONE>(v, t, m);
         const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
         if (st.active) {
             const int k = st.k;
@@ -1107,8 +1126,8 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
         long t = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
         if (t < v.P * (long)v.M) {
-            long p = ONE ? t : t / v.M;
-            int m = ONE ? 0 : (int)(t - p * v.M);
+            int m;
+            long p = split_member<ONE>(v, t, m);
             stage_path<REAL, ONE, BIF>(v, p, m, kh);
         }
     } else {
@@ -1117,8 +1136,8 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
         for (int q = 0; q < kBudgetTerms; ++q) bud[q] = 0.0;
         long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
         if (t < v.N * (long)v.M) {
-            long i = ONE ? t : t / v.M;
-            int m = ONE ? 0 : (int)(t - i * v.M);
+            int m;
+            long i = split_member<ONE>(v, t, m);
             stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud);
         }
         if (BUDGET) block_budget(bud, v.bpart, v.cell_blocks);
@@ -1137,8 +1156,7 @@ __global__ void __launch_bounds__(256) k_cfl(const Dev<REAL> v)
     int n_steps = 1;
     int m = 0;
     if (t < v.N * (long)v.M) {
-        long i = ONE ? t : t / v.M;
-        m = ONE ? 0 : (int)(t - i * v.M);
+        long i = split_member<ONE>(v, t, m);
         bool skip = RES && (v.flags[i] & CMF_CELL_DAM_RELATED);
         if (!skip) {
             REAL dist = v.dnd[i];
@@ -1231,7 +1249,8 @@ __global__ void __launch_bounds__(256) k_interval_end(const Dev<REAL> v)
 {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= v.N * (long)v.M) return;
-    int m = ONE ? 0 : (int)(t % v.M);
+    int m;
+    split_member<ONE>(v, t, m);
     if (v.nsub[m] & 1) {
         v.rs0[t] = v.rs1[t];
         v.fs0[t] = v.fs1[t];

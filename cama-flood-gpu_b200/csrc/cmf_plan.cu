@@ -155,6 +155,9 @@ void fill_dev(CmfPlan* p, const Layout& L)
     char* ws = (char*)v.workspace;
     d.N = (long)v.num_catchments;
     d.M = v.num_members;
+    d.mshift = -1;
+    for (int b = 0; b < 31; ++b)
+        if (v.num_members == (1 << b)) d.mshift = b;
     d.K = v.num_flood_levels;
     d.P = (long)v.num_bifurcation_paths;
     d.L = v.num_bifurcation_levels;
