@@ -168,6 +168,103 @@ def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15
     }
 
 
+def forcing_measure(device, net, desired_ids, steps: int = 24, grid_shape=(720, 1440),
+                    repeats: int = 10) -> dict:
+    """The forcing map in front of the path: a chunk of `steps` gridded runoff
+    fields (0.25-degree global grid, float32 mm/day) mapped onto the
+    workload's catchments (model order) by cmf_forcing_apply.  Kernel time by
+    CUDA events with the chunk resident; chunk e2e adds the pinned-host H2D
+    copy of the chunk; the CPU restatement (oracle scipy product) is timed
+    on one series and scaled."""
+    import torch
+    from cmfb200 import synthetic as syn
+    from cmfb200.forcing import apply_mapping, build_local_mapping, local_csr
+    from oracle import forcing as OF
+    tab = syn.runoff_mapping(net, grid_shape, seed=7)
+    m = build_local_mapping(tab, desired_ids, device)
+    chunk = torch.from_numpy(syn.gridded_runoff(grid_shape, steps, seed=3)).pin_memory()
+    dev = chunk.to(device)
+    out = torch.empty((steps, m.num_rows), dtype=torch.float32, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)     # > L2
+    stream = torch.cuda.current_stream(device)
+    for _ in range(3):
+        apply_mapping(m, dev, out=out, unit_factor=86400000.0)
+    times = []
+    for _ in range(repeats):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        apply_mapping(m, dev, out=out, unit_factor=86400000.0)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        times.append(a.elapsed_time(b))
+    ms = float(np.mean(times))
+    e2e = []
+    for _ in range(repeats):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        dev.copy_(chunk, non_blocking=True)
+        apply_mapping(m, dev, out=out, unit_factor=86400000.0)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        e2e.append(a.elapsed_time(b))
+    alg = m.bytes_per_launch(steps, 4, 4)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    rp, col, w, G = local_csr(tab, desired_ids)
+    g1 = chunk[0].numpy().reshape(1, -1).astype(np.float64)
+    t0 = time.perf_counter()
+    OF.scipy_map(rp, col, w, g1, G)
+    cpu_one = time.perf_counter() - t0
+    return {
+        "workload": f"{m.num_rows} catchments x {steps} steps, grid {grid_shape[0]}x{grid_shape[1]}, "
+                    f"nnz {m.nnz}",
+        "ms_per_chunk": ms, "ms_per_chunk_e2e": float(np.mean(e2e)),
+        "h2d_bytes_per_chunk": int(chunk.numel() * 4),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes": alg, "kernel": "k_forcing_map"},
+        "cpu_ms_per_chunk": cpu_one * steps * 1e3,
+        "cpu_sample": "one step of the chunk through scipy.sparse CSR (1 thread), x steps",
+    }
+
+
+def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: float,
+                        base_substeps: int) -> dict:
+    """The reference run scripts' output statistics ({"mean": total_outflow,
+    "last": river_depth}) accumulated in the interval graph: the same timed
+    intervals with and without them."""
+    import torch
+    spec = {"mean": ["total_outflow"], "last": ["river_depth"]}
+    model.set_variables_to_save(spec)
+    device = model.device
+    for k in range(2):
+        model.set_inputs(dev_forcing[first + k])
+        model.step_advance()
+    stream = torch.cuda.current_stream(device)
+    torch.cuda.synchronize(device)
+    counts = torch.zeros(steps, dtype=torch.int32, device=device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for j, k in enumerate(range(first, first + steps)):
+        model.set_inputs(dev_forcing[k])
+        model.step_advance()
+        counts[j].copy_(model.sub_step_counts()[0])
+    b.record(stream)
+    torch.cuda.synchronize(device)
+    ms = a.elapsed_time(b)
+    sub = int(counts.sum().item())
+    stats = model.collect_statistics()
+    ok = all(bool(torch.isfinite(v).all()) for v in stats.values())
+    model.set_variables_to_save(None)
+    with_ms = ms / max(sub, 1)
+    without_ms = base_ms / max(base_substeps, 1)
+    return {"variables_to_save": spec, "ms_per_substep": with_ms,
+            "ms_per_substep_without": without_ms, "overhead_frac": with_ms / without_ms - 1.0,
+            "sub_steps": sub, "finite": ok}
+
+
 def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -> dict:
     """The batched-ensemble workload at reduced size: `members` members of a
     `basins`-basin network (~`catchments` catchments per member, runoff and
@@ -530,6 +627,16 @@ def run_ours(args) -> None:
     e2e_value = float(w2.item()) / (float(t2.item()) / 1e3)
     model.check_status()
 
+    stats = None
+    if args.statistics:
+        # same forcing as the timed region (state has moved on; sub-step counts may differ)
+        stats = statistics_overhead(model, dev_forcing, args.warmup, args.steps, ms, substeps)
+
+    forcing_leg = None
+    if world == 1 and args.forcing_steps > 0:
+        forcing_leg = forcing_measure(device, net, model.base.catchment_id.cpu().numpy(),
+                                      steps=args.forcing_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(net, cfg, None)
@@ -569,6 +676,8 @@ def run_ours(args) -> None:
             "cpu_baseline": cpu,
             "ensemble": ensemble,
             "adjoint": adjoint,
+            "forcing": forcing_leg,
+            "statistics": stats,
             "clocks": clocks,
             "gpu_launches": launches,
         }
@@ -592,6 +701,10 @@ def main() -> None:
                     help="members of the batched-vs-looped comparison (0 skips it)")
     ap.add_argument("--adjoint-days", type=int, default=30,
                     help="daily intervals of the forward+adjoint comparison (0 = skip)")
+    ap.add_argument("--forcing-steps", type=int, default=24,
+                    help="steps per chunk of the gridded-runoff forcing map leg (0 = skip)")
+    ap.add_argument("--no-statistics", dest="statistics", action="store_false",
+                    help="skip the output-statistics overhead leg")
     ap.add_argument("--ensemble-catchments", type=int, default=600_000,
                     help="catchments per member of that comparison (the full workload has ~6M)")
     args = ap.parse_args()

@@ -20,7 +20,7 @@ CSRC = HERE / "csrc"
 INCLUDE = ROOT / "include"
 OUT_DIR = HERE / "cmfb200" / "lib"
 OUT = OUT_DIR / "libcmfb200.so"
-SOURCES = [CSRC / "cmf_plan.cu", CSRC / "cmf_adjoint.cu", CSRC / "cmf_topology.cpp"]
+SOURCES = [CSRC / "cmf_plan.cu", CSRC / "cmf_adjoint.cu", CSRC / "cmf_forcing.cu", CSRC / "cmf_topology.cpp"]
 DEPS = SOURCES + [CSRC / "cmf_device.cuh", INCLUDE / "cmfb200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -119,6 +119,20 @@ class CmfView(ctypes.Structure):
     ] + [(name, _P) for name in VIEW_POINTERS] + [("workspace_bytes", ctypes.c_size_t)]
 
 
+# output statistics (variables_to_save)
+STAT_VARIABLES = {
+    "river_outflow": 0, "flood_outflow": 1, "total_outflow": 2, "river_depth": 3,
+    "flood_depth": 4, "flood_fraction": 5, "protected_depth": 6, "river_storage": 7,
+    "flood_storage": 8, "protected_storage": 9,
+}
+STAT_OPS = {"mean": 0, "max": 1, "min": 2, "last": 3}
+MAX_STATISTICS = 16
+
+
+class CmfStatistic(ctypes.Structure):
+    _fields_ = [("variable", _I32), ("op", _I32), ("out", _P)]
+
+
 class CmfError(RuntimeError):
     """A libcmfb200 entry point returned a non-zero status."""
 
@@ -169,6 +183,14 @@ def lib() -> ctypes.CDLL:
     h.cmf_substep_noalloc.argtypes = [ctypes.POINTER(CmfView), _P, ctypes.c_int]
     h.cmf_budget_flush.restype = ctypes.c_int
     h.cmf_budget_flush.argtypes = [_P, _P]
+    h.cmf_stats_attach.restype = ctypes.c_int
+    h.cmf_stats_attach.argtypes = [_P, ctypes.c_int, ctypes.POINTER(CmfStatistic), _P]
+    h.cmf_stats_reset.restype = ctypes.c_int
+    h.cmf_stats_reset.argtypes = [_P, _P]
+    h.cmf_stats_accumulate.restype = ctypes.c_int
+    h.cmf_stats_accumulate.argtypes = [_P, _P, _I32]
+    h.cmf_stats_finalize.restype = ctypes.c_int
+    h.cmf_stats_finalize.argtypes = [_P, _P]
     for name, args in {
         "cmf_topo_topological_sort": [_I64, _P, _P, _P],
         "cmf_topo_upstream_csr": [_I64, _P, _P, _P],

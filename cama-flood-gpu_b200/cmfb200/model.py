@@ -127,6 +127,11 @@ class CaMaFlood:
     mode; "float64"), `num_members` (ensemble members, member-innermost),
     `batched_fields` (per-member parameters), `max_sub_step_seconds` (an
     optional CFL dt cap), `use_cuda_graph` and `budget` (fp64 water budget).
+    `variables_to_save` takes the reference's form ({"mean": ["total_outflow"],
+    "last": ["river_depth"]}, scripts/run_daily_bin.py:28) and accumulates
+    those statistics on the device after every sub-step; `collect_statistics()`
+    ends an output period (no file writer: the reference's NetCDF output
+    workers are outside this path).
     """
 
     def __init__(self, device: str | torch.device = "cuda", input_proxy: Optional[Mapping] = None,
@@ -136,7 +141,8 @@ class CaMaFlood:
                  BLOCK_SIZE: int = 256, use_cuda_graph: bool = True,
                  max_sub_step_seconds: float = 0.0, max_sub_steps_cap: int = 0,
                  gravity: float = 9.8, min_kinematic_slope: float = 1.0e-5,
-                 adaptive_time_factor: float = 0.7, budget: bool = False):
+                 adaptive_time_factor: float = 0.7, budget: bool = False,
+                 variables_to_save: Optional[Mapping[str, Iterable[str]]] = None):
         if input_proxy is None:
             raise ValueError("input_proxy (field name -> array mapping) is required")
         mods = set(opened_modules) | {"base"}
@@ -166,7 +172,9 @@ class CaMaFlood:
         self._plan = None
         self._prepare(dict(input_proxy), dict(batched_fields or {}))
         self._upload()
+        self._init_statistics(variables_to_save or {})
         self._create_plan()
+        self.reset_statistics()
 
     # ------------------------------------------------------------------ #
     # construction
@@ -540,6 +548,73 @@ class CaMaFlood:
         plan = ctypes.c_void_p()
         _lib.check(lib.cmf_plan_create(ctypes.byref(view), ctypes.byref(plan)), "plan_create")
         self._plan = plan
+        self._attach_statistics()
+
+    # ------------------------------------------------------------------ #
+    # output statistics (variables_to_save)
+    # ------------------------------------------------------------------ #
+    def _init_statistics(self, spec: Mapping[str, Iterable[str]]) -> None:
+        items = []
+        for op, names in spec.items():
+            if op not in _lib.STAT_OPS:
+                raise ValueError(f"statistic '{op}' is not supported (one of {sorted(_lib.STAT_OPS)})")
+            for name in ([names] if isinstance(names, str) else list(names)):
+                if name not in _lib.STAT_VARIABLES:
+                    raise ValueError(f"variable '{name}' cannot be saved "
+                                     f"(one of {sorted(_lib.STAT_VARIABLES)})")
+                if name.startswith("protected") and not self.has.lev:
+                    raise ValueError(f"'{name}' needs the levee module")
+                if (name, op) not in items:
+                    items.append((name, op))
+        if len(items) > _lib.MAX_STATISTICS:
+            raise ValueError(f"at most {_lib.MAX_STATISTICS} statistics")
+        self._stats_spec = items
+        shape = tuple(self.base.river_depth.shape)
+        self._stats_out = {f"{n}_{o}": torch.zeros(shape, dtype=torch.float64, device=self.device)
+                           for n, o in items}
+        self._stats_weight = torch.zeros(self.num_members, dtype=torch.float64, device=self.device)
+
+    def _attach_statistics(self) -> None:
+        arr = (_lib.CmfStatistic * max(len(self._stats_spec), 1))()
+        for q, (name, op) in enumerate(self._stats_spec):
+            arr[q].variable = _lib.STAT_VARIABLES[name]
+            arr[q].op = _lib.STAT_OPS[op]
+            arr[q].out = self._stats_out[f"{name}_{op}"].data_ptr()
+        _lib.check(_lib.lib().cmf_stats_attach(self._plan, len(self._stats_spec), arr,
+                                               self._stats_weight.data_ptr()), "stats_attach")
+
+    def set_variables_to_save(self, spec: Optional[Mapping[str, Iterable[str]]]) -> None:
+        """Replace the saved statistics (None or {} saves none) and start a new
+        output period; the interval graph is rebuilt on the next step."""
+        self._init_statistics(spec or {})
+        self._attach_statistics()
+        self.reset_statistics()
+
+    @property
+    def variables_to_save(self) -> dict[str, list[str]]:
+        out: dict[str, list[str]] = {}
+        for name, op in self._stats_spec:
+            out.setdefault(op, []).append(name)
+        return out
+
+    def reset_statistics(self) -> None:
+        """Start an output period (MEAN -> 0, MAX -> -inf, MIN -> +inf)."""
+        _lib.check(_lib.lib().cmf_stats_reset(self._plan, self._stream()), "stats_reset")
+
+    def accumulate_statistics(self, k: int) -> None:
+        """Fold sub-step k run through the per-phase entry points into the
+        statistics (step_advance does this itself)."""
+        _lib.check(_lib.lib().cmf_stats_accumulate(self._plan, self._stream(), int(k)),
+                   "stats_accumulate")
+
+    def collect_statistics(self, reset: bool = True) -> dict[str, torch.Tensor]:
+        """End the output period: {"<variable>_<op>": fp64 device tensor in
+        model order ([N] or [N, M])}, then start the next one."""
+        _lib.check(_lib.lib().cmf_stats_finalize(self._plan, self._stream()), "stats_finalize")
+        out = {k: v.clone() for k, v in self._stats_out.items()}
+        if reset:
+            self.reset_statistics()
+        return out
 
     # ------------------------------------------------------------------ #
     # public API (cama_flood_model.py:74-173)

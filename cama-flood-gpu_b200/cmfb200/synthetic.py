@@ -274,3 +274,59 @@ def ensemble_factors(num_catchments: int, members: int, seed: int = 0):
     runoff = np.exp(0.3 * rng.standard_normal((num_catchments, members))).astype(np.float32)
     manning = rng.uniform(0.8, 1.2, size=(num_catchments, members)).astype(np.float32)
     return runoff, manning
+
+
+def runoff_mapping(network: Network, grid_shape=(720, 1440), seed: int = 0, max_cells: int = 4,
+                   extra_rows: int = 0) -> dict:
+    """A runoff mapping table in the reference's `.npz` layout
+    (cmfgpu/params/export_bin.py:955-983) for `network` on a ny x nx runoff
+    grid: every catchment draws 1..max_cells cells of the 2x2 block at its grid
+    position (catchments sweep the grid in generator order, so neighbours in
+    the river tree share nearby cells), weights split its area.  Rows are
+    shuffled against the network order and `extra_rows` rows for catchments
+    outside the network are added, as a global table seen by one domain."""
+    rng = np.random.default_rng([seed, 271828])
+    ids = np.asarray(network.fields["catchment_id"], dtype=np.int64)
+    area = np.asarray(network.fields["catchment_area"], dtype=np.float64)
+    n = ids.size + int(extra_rows)
+    ny, nx = int(grid_shape[0]), int(grid_shape[1])
+    G = ny * nx
+    all_ids = np.concatenate([ids, ids.max(initial=-1) + 1 + np.arange(int(extra_rows))])
+    all_area = np.concatenate([area, rng.uniform(5e7, 5e8, size=int(extra_rows))])
+    base = (np.arange(n, dtype=np.int64) * G) // max(n, 1)
+    bx, by = base % nx, base // nx
+    cnt = rng.integers(1, max_cells + 1, size=n)
+    offs = np.array([[0, 0], [1, 0], [0, 1], [1, 1]], dtype=np.int64)
+    perm = np.argsort(rng.random((n, 4)), axis=1)          # which block cells, in which order
+    rows = np.repeat(np.arange(n), cnt)
+    slot = np.arange(rows.size) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    o = offs[perm[rows, slot % 4]]
+    cx = np.minimum(bx[rows] + o[:, 0], nx - 1)
+    cy = np.minimum(by[rows] + o[:, 1], ny - 1)
+    frac = rng.gamma(2.0, 1.0, size=rows.size)
+    frac /= np.bincount(rows, weights=frac, minlength=n)[rows]
+    data = all_area[rows] * frac
+    order = rng.permutation(n)                             # table row order
+    lens = cnt[order]
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=indptr[1:])
+    starts = np.cumsum(cnt) - cnt
+    take = np.repeat(starts[order], lens) + (np.arange(indptr[-1]) - np.repeat(indptr[:-1], lens))
+    return {
+        "catchment_ids": all_ids[order],
+        "sparse_data": data[take],
+        "sparse_indices": (cy * nx + cx)[take].astype(np.int64),
+        "sparse_indptr": indptr,
+        "matrix_shape": np.array([n, G], dtype=np.int64),
+        "coord_lon": np.linspace(-180 + 180 / nx, 180 - 180 / nx, nx),
+        "coord_lat": np.linspace(90 - 90 / ny, -90 + 90 / ny, ny),
+    }
+
+
+def gridded_runoff(grid_shape, steps: int, seed: int = 0, members: int = 0) -> np.ndarray:
+    """Raw gridded runoff in mm/day (gamma k=0.5, mean 2 mm/day), float32
+    [steps, ny, nx] (or [steps, members, ny, nx]); unit_factor 86400000 maps
+    mm/day x m^2 to m^3/s, as in the reference's daily-bin runs."""
+    rng = np.random.default_rng([seed, 161803])
+    shape = (steps, members, *grid_shape) if members else (steps, *grid_shape)
+    return rng.gamma(0.5, 4.0, size=shape).astype(np.float32)

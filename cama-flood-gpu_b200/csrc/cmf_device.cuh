@@ -1290,4 +1290,94 @@ __global__ void k_budget_flush(double* bpart, int nblocks, double* budget, const
     if (threadIdx.x == 0 && count_steps) budget[CMF_BUDGET_SUBSTEPS] += (double)ctl[kCtlMaxSteps];
 }
 
+// ---------------------------------------------------------------------------
+// Output statistics (the reference's variables_to_save), folded in after each
+// sub-step by one elementwise kernel at the end of the sub-step.
+// ---------------------------------------------------------------------------
+struct StatsArgs {
+    int count;
+    int need_weight;
+    int var[CMF_MAX_STATISTICS];
+    int op[CMF_MAX_STATISTICS];
+    double* out[CMF_MAX_STATISTICS];
+    double* weight;
+};
+
+// Value of a statistics variable at element t.  `after` selects the storage
+// buffer: the state after sub-step k (k >= 0, the ping-pong destination of
+// k) or the interval state (k < 0, after k_interval_end).  Cells without a
+// levee carry protected depth == flood depth (k_stage writes that only on the
+// member's last sub-step, so it is taken from the flood depth here).
+template <typename REAL>
+__device__ __forceinline__ double stat_value(const Dev<REAL>& v, int var, long t, long i, int k)
+{
+    const bool second = k >= 0 && !(k & 1);
+    switch (var) {
+    case CMF_VAR_RIVER_OUTFLOW: return (double)v.rout[t];
+    case CMF_VAR_FLOOD_OUTFLOW: return (double)v.fout[t];
+    case CMF_VAR_TOTAL_OUTFLOW: return __dadd_rn((double)v.rout[t], (double)v.fout[t]);
+    case CMF_VAR_RIVER_DEPTH: return (double)v.rdep[t];
+    case CMF_VAR_FLOOD_DEPTH: return (double)v.fdep[t];
+    case CMF_VAR_FLOOD_FRACTION: return (double)v.ffr[t];
+    case CMF_VAR_PROTECTED_DEPTH:
+        return (v.flags[i] & CMF_CELL_LEVEE) ? (double)v.pdep[t] : (double)v.fdep[t];
+    case CMF_VAR_RIVER_STORAGE: return second ? v.rs1[t] : v.rs0[t];
+    case CMF_VAR_FLOOD_STORAGE: return second ? v.fs1[t] : v.fs0[t];
+    case CMF_VAR_PROTECTED_STORAGE: return (v.flags[i] & CMF_CELL_LEVEE) ? v.ps[t] : 0.0;
+    default: return 0.0;
+    }
+}
+
+// kh >= 0: host step index; kh == -1: the step that the last kernel of the
+// sub-step just finished (the device counter was advanced by it).
+template <typename REAL, bool ONE>
+__global__ void __launch_bounds__(256) k_stats_accumulate(const Dev<REAL> v, const StatsArgs a, int kh)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= v.N * (long)v.M) return;
+    int m;
+    const long i = split_member<ONE>(v, t, m);
+    const int k = kh >= 0 ? kh : v.ctl[kCtlStep] - 1;
+    if (k >= v.nsub[m]) return;  // member idle in this sub-step
+    const double dt = (double)v.dt[m];
+    if (a.need_weight && i == 0) a.weight[m] = __dadd_rn(a.weight[m], dt);
+#pragma unroll 1
+    for (int q = 0; q < a.count; ++q) {
+        const int op = a.op[q];
+        if (op == CMF_STAT_LAST) continue;
+        const double x = stat_value(v, a.var[q], t, i, k);
+        double* o = a.out[q] + t;
+        const double acc = *o;
+        if (op == CMF_STAT_MEAN) *o = __dadd_rn(acc, __dmul_rn(x, dt));
+        else if (op == CMF_STAT_MAX) *o = (x > acc || x != x) ? x : acc;
+        else *o = (x < acc || x != x) ? x : acc;
+    }
+}
+
+template <typename REAL, bool ONE>
+__global__ void __launch_bounds__(256) k_stats_reset(const Dev<REAL> v, const StatsArgs a)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < v.M && a.weight) a.weight[t] = 0.0;
+    if (t >= v.N * (long)v.M) return;
+    for (int q = 0; q < a.count; ++q) {
+        const int op = a.op[q];
+        a.out[q][t] = op == CMF_STAT_MAX ? -INFINITY : (op == CMF_STAT_MIN ? INFINITY : 0.0);
+    }
+}
+
+template <typename REAL, bool ONE>
+__global__ void __launch_bounds__(256) k_stats_finalize(const Dev<REAL> v, const StatsArgs a)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= v.N * (long)v.M) return;
+    int m;
+    const long i = split_member<ONE>(v, t, m);
+    for (int q = 0; q < a.count; ++q) {
+        const int op = a.op[q];
+        if (op == CMF_STAT_MEAN) a.out[q][t] = a.out[q][t] / a.weight[m];
+        else if (op == CMF_STAT_LAST) a.out[q][t] = stat_value(v, a.var[q], t, i, -1);
+    }
+}
+
 }  // namespace cmf

@@ -38,6 +38,9 @@ struct KernelSet {
     const void* copy_back;
     const void* limit;
     const void* levee;
+    const void* stats_acc;
+    const void* stats_reset;
+    const void* stats_fin;
 };
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUD>
@@ -53,6 +56,9 @@ KernelSet make_set()
     k.copy_back = (const void*)k_copy_back<REAL, ONE>;
     k.limit = (const void*)k_limit<REAL, ONE, BIF>;
     k.levee = (const void*)k_levee<REAL, ONE>;
+    k.stats_acc = (const void*)k_stats_accumulate<REAL, ONE>;
+    k.stats_reset = (const void*)k_stats_reset<REAL, ONE>;
+    k.stats_fin = (const void*)k_stats_finalize<REAL, ONE>;
     return k;
 }
 
@@ -142,6 +148,8 @@ struct CmfPlan {
     cudaGraphConditionalHandle cond;
     double graph_T;
     int graph_fixed;
+    // output statistics folded in after every sub-step (count == 0: none)
+    StatsArgs stats;
 };
 
 namespace {
@@ -370,12 +378,21 @@ int build_graph(CmfPlan* p, double T, int fixed_n)
         int set = 1;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
         if ((rc = add_kernel(&b2, body, &bl, 1, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
+        cudaGraphNode_t last = b2;
         if (p->levee_blocks > 0) {
             cudaGraphNode_t b3;
             int adv = 1;
             void* a3[] = {p->dev, &kh, &fd, &h, &adv};
             if ((rc = add_kernel(&b3, body, &b2, 1, p->ks.levee, p->levee_blocks, p->tpb, a3)) != CMF_OK)
                 goto fail;
+            last = b3;
+        }
+        if (p->stats.count > 0) {
+            // after the advancing kernel: reads step counter - 1
+            cudaGraphNode_t b4;
+            void* a4[] = {p->dev, &p->stats, &kh};
+            const int sb = ceil_div((long)v.num_catchments * v.num_members, 256);
+            if ((rc = add_kernel(&b4, body, &last, 1, p->ks.stats_acc, sb, 256, a4)) != CMF_OK) goto fail;
         }
     }
     {
@@ -460,6 +477,11 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
         if ((rc = launch(p->ks.stage, grid, p->tpb, a2, s)) != CMF_OK) return rc;
         if (p->levee_blocks > 0) {
             if ((rc = launch(p->ks.levee, p->levee_blocks, p->tpb, a2, s)) != CMF_OK) return rc;
+        }
+        if (p->stats.count > 0) {
+            void* a4[] = {p->dev, &p->stats, &kh};
+            const int sb = ceil_div((long)v.num_catchments * v.num_members, 256);
+            if ((rc = launch(p->ks.stats_acc, sb, 256, a4, s)) != CMF_OK) return rc;
         }
     }
     {
@@ -765,6 +787,65 @@ int cmf_budget_flush(CmfPlan* p, void* stream)
     int cs = 0;
     void* args[] = {&bpart, &nb, &budget, &ctl, &cs};
     return launch((const void*)k_budget_flush, 1, 256, args, (cudaStream_t)stream);
+}
+
+int cmf_stats_attach(CmfPlan* p, int count, const CmfStatistic* stats, double* weight)
+{
+    if (!p || count < 0 || count > CMF_MAX_STATISTICS) return CMF_ERR_ARG;
+    if (count > 0 && !stats) return CMF_ERR_ARG;
+    StatsArgs a;
+    std::memset(&a, 0, sizeof(a));
+    const bool lev = p->view.features & CMF_FEAT_LEVEE;
+    for (int q = 0; q < count; ++q) {
+        const int var = stats[q].variable, op = stats[q].op;
+        if (var < 0 || var >= CMF_VAR_COUNT || op < CMF_STAT_MEAN || op > CMF_STAT_LAST) return CMF_ERR_ARG;
+        if (!stats[q].out) return CMF_ERR_ARG;
+        if ((var == CMF_VAR_PROTECTED_DEPTH || var == CMF_VAR_PROTECTED_STORAGE) && !lev)
+            return CMF_ERR_ARG;
+        a.var[q] = var;
+        a.op[q] = op;
+        a.out[q] = stats[q].out;
+        if (op == CMF_STAT_MEAN) a.need_weight = 1;
+    }
+    if (a.need_weight && !weight) return CMF_ERR_ARG;
+    a.count = count;
+    a.weight = weight;
+    // the sub-step body changes: drop the graph once no launch of it is in flight
+    if (p->graph_ready) {
+        const int rc = check_cuda(cudaDeviceSynchronize());
+        if (rc != CMF_OK) return rc;
+    }
+    destroy_graph(p);
+    p->stats = a;
+    return CMF_OK;
+}
+
+int cmf_stats_reset(CmfPlan* p, void* stream)
+{
+    if (!p) return CMF_ERR_ARG;
+    if (p->stats.count == 0) return CMF_OK;
+    void* args[] = {p->dev, &p->stats};
+    return launch(p->ks.stats_reset, ceil_div((long)p->view.num_catchments * p->view.num_members, 256),
+                  256, args, (cudaStream_t)stream);
+}
+
+int cmf_stats_accumulate(CmfPlan* p, void* stream, int32_t k)
+{
+    if (!p || k < 0) return CMF_ERR_ARG;
+    if (p->stats.count == 0) return CMF_OK;
+    int kh = k;
+    void* args[] = {p->dev, &p->stats, &kh};
+    return launch(p->ks.stats_acc, ceil_div((long)p->view.num_catchments * p->view.num_members, 256),
+                  256, args, (cudaStream_t)stream);
+}
+
+int cmf_stats_finalize(CmfPlan* p, void* stream)
+{
+    if (!p) return CMF_ERR_ARG;
+    if (p->stats.count == 0) return CMF_OK;
+    void* args[] = {p->dev, &p->stats};
+    return launch(p->ks.stats_fin, ceil_div((long)p->view.num_catchments * p->view.num_members, 256),
+                  256, args, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -284,6 +284,101 @@ int cmf_substep_noalloc(const CmfView* view, void* stream, int diag);
 /* Reduce the per-CTA budget partials into view.budget and clear them. */
 int cmf_budget_flush(CmfPlan* plan, void* stream);
 
+/* ---- output statistics accumulated on the device -------------------------
+ * The reference's `variables_to_save` (scripts/run_daily_bin.py:28, e.g.
+ * {"mean": ["total_outflow"], "last": ["river_depth"]}) aggregated by its
+ * output layer outside the step.  Here the aggregation is one kernel appended
+ * to the sub-step inside the interval graph, so a whole output period runs
+ * without a device-to-host copy.  Conventions:
+ *   MEAN  sum over sub-steps of value * dt, divided at finalize by the sum
+ *         of dt of the member (a time average over the output period);
+ *   MAX / MIN  over the values after every sub-step (NaN sticks);
+ *   LAST  the value at finalize time.
+ * Products and sums are rounded separately (no fused multiply-add), in the
+ * order of the sub-steps, so a host replay with separate fp64 ops matches
+ * bit for bit.  Accumulators are caller-owned fp64 arrays of N x M elements
+ * in the state layout; `weight` is a caller-owned fp64 array of M elements. */
+#define CMF_VAR_RIVER_OUTFLOW 0
+#define CMF_VAR_FLOOD_OUTFLOW 1
+#define CMF_VAR_TOTAL_OUTFLOW 2 /* river + flood outflow (base.py:412-419)  */
+#define CMF_VAR_RIVER_DEPTH 3
+#define CMF_VAR_FLOOD_DEPTH 4
+#define CMF_VAR_FLOOD_FRACTION 5
+#define CMF_VAR_PROTECTED_DEPTH 6
+#define CMF_VAR_RIVER_STORAGE 7
+#define CMF_VAR_FLOOD_STORAGE 8
+#define CMF_VAR_PROTECTED_STORAGE 9
+#define CMF_VAR_COUNT 10
+
+#define CMF_STAT_MEAN 0
+#define CMF_STAT_MAX 1
+#define CMF_STAT_MIN 2
+#define CMF_STAT_LAST 3
+
+#define CMF_MAX_STATISTICS 16
+
+typedef struct CmfStatistic {
+    int32_t variable; /* CMF_VAR_*  */
+    int32_t op;       /* CMF_STAT_* */
+    double* out;      /* [N * M] device accumulator / result */
+} CmfStatistic;
+
+/* Attach `count` statistics to the plan (count == 0 detaches).  The interval
+ * graph is rebuilt on the next cmf_step_interval.  Protected fields need the
+ * levee module. */
+int cmf_stats_attach(CmfPlan* plan, int count, const CmfStatistic* stats,
+                     double* weight);
+/* Start an output period: MEAN -> 0, MAX -> -inf, MIN -> +inf, weight -> 0. */
+int cmf_stats_reset(CmfPlan* plan, void* stream);
+/* Fold the sub-step that the per-phase entry points just finished (host step
+ * index k, as in cmf_launch_substep) into the statistics. */
+int cmf_stats_accumulate(CmfPlan* plan, void* stream, int32_t k);
+/* End an output period: MEAN /= weight, LAST := the current value. */
+int cmf_stats_finalize(CmfPlan* plan, void* stream);
+
+/* ---- runoff forcing map: gridded runoff -> catchments --------------------
+ * Replaces the forcing step before the routing path: hydroforge's
+ * `dataset.build_local_mapping(mapping_file, desired_catchment_ids, device)`
+ * and `dataset.shard_forcing(chunk, local_mapping)`
+ * (scripts/run_daily_bin.py:98-118).  The mapping is the reference's runoff
+ * mapping table (`.npz`: catchment_ids, sparse_data, sparse_indices,
+ * sparse_indptr, matrix_shape; read in cmfgpu/params/export_bin.py:955-983)
+ * restricted to the model's catchments, rows in model order, columns the
+ * flattened runoff grid index iy * nx + ix (export_bin.py:1071-1075),
+ * weights in m^2.  For every catchment row r, step t and member m:
+ *   out[t, r, m] = (sum_k w_k * grid[t, m, col_k]) * (1 / unit_factor)
+ * summed in entry order in fp64 with products and sums rounded separately;
+ * the reciprocal of unit_factor is rounded once on the host.
+ * CMF_FORCING_SKIP_MISSING leaves out entries whose grid value is NaN or
+ * equals missing_value (compared in the grid's dtype);
+ * CMF_FORCING_CLAMP_NEGATIVE sets negative sums to zero.  A column outside
+ * [0, num_cols) is skipped and sets CMF_STATUS_BAD_INDEX in *status (when
+ * status is not NULL). */
+#define CMF_DTYPE_F32 0
+#define CMF_DTYPE_F64 1
+#define CMF_FORCING_SKIP_MISSING 1
+#define CMF_FORCING_CLAMP_NEGATIVE 2
+#define CMF_STATUS_BAD_INDEX 4
+
+typedef struct CmfForcingMap {
+    int64_t num_rows;       /* catchments (model order)                */
+    int64_t num_cols;       /* runoff grid cells (ny * nx)             */
+    const int64_t* row_ptr; /* [num_rows + 1] device                   */
+    const int32_t* col;     /* [nnz] device                            */
+    const double* weight;   /* [nnz] device, m^2                       */
+} CmfForcingMap;
+
+/* grid: element (t, m, c) at grid[t * grid_step_stride + m * grid_member_stride
+ * + c]; out: element (t, r, m) at out[t * out_step_strides + m *
+ * out_member_stride + r * out_row_stride] (strides in elements). */
+int cmf_forcing_apply(const CmfForcingMap* map, void* stream, const void* grid,
+                      int grid_dtype, int32_t steps, int32_t members,
+                      int64_t grid_step_stride, int64_t grid_member_stride,
+                      void* out, int out_dtype, int64_t out_step_stride,
+                      int64_t out_member_stride, int64_t out_row_stride,
+                      double unit_factor, double missing_value, int flags,
+                      int* status);
+
 /* ---- adjoint of the sub-step (no counterpart in the reference) -----------
  * Reverse mode of the routing sub-step in fp64, every physics module, for
  * gradients of a loss on discharge with respect to the Manning coefficients,
