@@ -5,6 +5,7 @@ names, `set_inputs`, `step_advance`); all compute runs in libcmfb200.so
 (hand-written CUDA kernels behind a C ABI, include/cmfb200.h).
 """
 from .model import CaMaFlood, InputProxy, Module  # noqa: F401
+from .prefetch import InputPrefetcher  # noqa: F401
 from . import synthetic, topology  # noqa: F401
 
-__all__ = ["CaMaFlood", "InputProxy", "Module", "synthetic", "topology"]
+__all__ = ["CaMaFlood", "InputProxy", "InputPrefetcher", "Module", "synthetic", "topology"]
