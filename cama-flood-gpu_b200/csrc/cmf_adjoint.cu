@@ -54,6 +54,7 @@
 #include <cstdint>
 #include <cstring>
 #include <new>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace {
@@ -166,8 +167,13 @@ struct Ctx {
     // bifurcation
     const int *bptr, *bpaths, *bci, *bdi;
     const double *bman, *bwid, *blen, *belv;
-    // slot geometry (doubles)
-    long slot_len, path_off;
+    // dam cells (reservoir or dam-upstream), compact
+    long ND;
+    const int* dam;
+    // slot geometry (doubles); lev_off: the pre-levee stage of the levee
+    // cells [4][NLV] (river/flood storage, river/flood depth) that ka_levee
+    // records in the slot of its sub-step for kr_levee_prep
+    long slot_len, path_off, lev_off;
     int grid_cells, grid_paths;
 };
 
@@ -446,17 +452,21 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
 // Contract the Jacobian of a templated branch with output adjoints:
 // in_bar[j] += sum_o out_bar[o] * d out[o] / d in[j], one dual pass per input.
 template <int NI, int NO, typename F>
+__device__ __forceinline__ double vjp_column(const double* in, const double* out_bar, int j, F f)
+{
+    Dual x[NI];
+    for (int q = 0; q < NI; ++q) x[q] = {in[q], q == j ? 1.0 : 0.0};
+    Dual y[NO];
+    f(x, y);
+    double s = 0.0;
+    for (int o = 0; o < NO; ++o) s += out_bar[o] * y[o].d;
+    return s;
+}
+
+template <int NI, int NO, typename F>
 __device__ __forceinline__ void vjp(const double* in, const double* out_bar, double* in_bar, F f)
 {
-    for (int j = 0; j < NI; ++j) {
-        Dual x[NI];
-        for (int q = 0; q < NI; ++q) x[q] = {in[q], q == j ? 1.0 : 0.0};
-        Dual y[NO];
-        f(x, y);
-        double s = 0.0;
-        for (int o = 0; o < NO; ++o) s += out_bar[o] * y[o].d;
-        in_bar[j] += s;
-    }
+    for (int j = 0; j < NI; ++j) in_bar[j] += vjp_column<NI, NO>(in, out_bar, j, f);
 }
 
 // ---------------------------------------------------------------------------
@@ -904,7 +914,7 @@ __global__ void __launch_bounds__(kBlock) ka_stage(const Ctx c, const double* X,
 
 // Levee re-partition of the levee cells (levee.cu:29-261) on the flood-stage
 // result ka_stage left in Y, over the compact levee list.
-__global__ void __launch_bounds__(kBlock) ka_levee(const Ctx c, double* Y)
+__global__ void __launch_bounds__(kBlock) ka_levee(const Ctx c, double* X, double* Y)
 {
     const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= c.NLV) return;
@@ -912,6 +922,9 @@ __global__ void __launch_bounds__(kBlock) ka_levee(const Ctx c, double* Y)
     const long i = c.lci[l];
     const double in[6] = {Y[F_RS * N + i], Y[F_FS * N + i], Y[F_RDEP * N + i], Y[F_FDEP * N + i],
                           c.rw[i], c.rh[i]};
+    double* rec = X + c.lev_off;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rec[k * c.NLV + l] = in[k];
     double out[6], ffr = 0.0;
     levee_part<double>(c, i, in, ffr, out);
     Y[F_RS * N + i] = out[0];
@@ -1010,16 +1023,13 @@ __global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const doubl
     const long i = c.lci[l];
     apply_pending(c, i, a);
     const double* lam = a.lam;
-    Store t;
-    gather_inflow(c, X, i, t);
-    const double tot = store_eval(X[F_RS * N + i], X[F_FS * N + i], X[F_PS * N + i], runoff[i], dt, t);
-    Stage s;
-    stage_eval(c, i, tot, c.rh[i], c.rw[i], c.rl[i], s);
+    // the flood-stage result the levee re-partitioned, recorded by ka_levee
+    const double* rec = X + c.lev_off;
     double* q = levin(c, a.scr) + 10 * l;
-    q[0] = s.rs;
-    q[1] = s.fs;
-    q[2] = s.rdep;
-    q[3] = s.fdep;
+    q[0] = rec[l];
+    q[1] = rec[c.NLV + l];
+    q[2] = rec[2 * c.NLV + l];
+    q[3] = rec[3 * c.NLV + l];
     q[4] = lam[F_RS * N + i];
     q[5] = lam[F_FS * N + i];
     q[6] = lam[F_PS * N + i];
@@ -1451,46 +1461,52 @@ __device__ __forceinline__ void flux_bars(const Ctx& c, const double* X, const A
 }
 
 // Reservoir release and dam-upstream kinematic flow reversed (kr_dam), one
-// thread per cell (the others return at once), after kr_momentum: it adds to
+// thread per dam cell and input direction (one dual pass each; the
+// directions of a cell write distinct fields), after kr_momentum: it adds to
 // what kr_momentum wrote.
+constexpr int kDamDirs = 7;
+
 __global__ void __launch_bounds__(kBlock) kr_dam(const Ctx c, const double* X,
                                                  const double* runoff, double dt, Adj a)
 {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.N) return;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.ND * (long)kDamDirs) return;
+    const long d = t / kDamDirs;
+    const int j = (int)(t - d * kDamDirs);
+    const long i = c.dam[d];
     const uint8_t fl = c.flags[i];
-    if (!(fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) return;
     const long N = c.N;
     double* lam = a.lam;
     double qr_bar, qf_bar;
     flux_bars(c, X, a, i, dt, qr_bar, qf_bar);
     if (fl & CMF_CELL_RESERVOIR) {
+        if (j >= 4) return;
         const double in[4] = {X[F_RS * N + i], X[F_FS * N + i], X[F_RTI * N + i], runoff[i]};
         const double ob[1] = {qr_bar};
-        double ib[4] = {0, 0, 0, 0};
         const int slot = c.rslot[i];
-        vjp<4, 1>(in, ob, ib, [&](const Dual* x, Dual* y) {
+        const double ib = 0.0 + vjp_column<4, 1>(in, ob, j, [&](const Dual* x, Dual* y) {
             y[0] = release<Dual>(c, slot, x[0], x[1], x[2], x[3], dt);
         });
-        lam[F_RS * N + i] += ib[0];
-        lam[F_FS * N + i] += ib[1];
-        lam[F_RTI * N + i] += ib[2];
-        a.groff[i] += ib[3];
+        double* dst = j == 0 ? lam + F_RS * N : j == 1 ? lam + F_FS * N : j == 2 ? lam + F_RTI * N : a.groff;
+        dst[i] += ib;
     } else {
         const double in[7] = {X[F_RDEP * N + i], X[F_FDEP * N + i], X[F_RS * N + i],
                               X[F_FS * N + i], c.rw[i], c.rman[i], c.fman[i]};
         const double ob[2] = {qr_bar, qf_bar};
-        double ib[7] = {0, 0, 0, 0, 0, 0, 0};
-        vjp<7, 2>(in, ob, ib, [&](const Dual* x, Dual* y) {
+        const double ib = 0.0 + vjp_column<7, 2>(in, ob, j, [&](const Dual* x, Dual* y) {
             kinematic<Dual>(c, i, x[0], x[1], x[2], x[3], x[4], x[5], x[6], dt, y[0], y[1]);
         });
-        lam[F_RDEP * N + i] += ib[0];
-        lam[F_FDEP * N + i] += ib[1];
-        lam[F_RS * N + i] += ib[2];
-        lam[F_FS * N + i] += ib[3];
-        a.grad[G_RW * N + i] += ib[4];
-        a.grad[G_RMAN * N + i] += ib[5];
-        a.grad[G_FMAN * N + i] += ib[6];
+        double* dst;
+        switch (j) {
+        case 0: dst = lam + F_RDEP * N; break;
+        case 1: dst = lam + F_FDEP * N; break;
+        case 2: dst = lam + F_RS * N; break;
+        case 3: dst = lam + F_FS * N; break;
+        case 4: dst = a.grad + G_RW * N; break;
+        case 5: dst = a.grad + G_RMAN * N; break;
+        default: dst = a.grad + G_FMAN * N; break;
+        }
+        dst[i] += ib;
     }
 }
 
@@ -1507,6 +1523,7 @@ __global__ void __launch_bounds__(kBlock) kr_finalize(const Ctx c, Adj a)
 struct CmfAdjPlan {
     Ctx ctx;
     int grid;
+    int* dam_list;  // device, ctx.ND entries
 };
 
 namespace {
@@ -1625,7 +1642,33 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
         c.belv = static_cast<const double*>(v->bifurcation_elevation);
     }
     c.path_off = (long)kSlotCell * c.N;
-    c.slot_len = c.path_off + 3L * c.P * c.L + 2 * c.P;
+    c.lev_off = c.path_off + 3L * c.P * c.L + 2 * c.P;
+    c.slot_len = c.lev_off + 4L * c.NLV;
+    if (res) {
+        // compact list of the dam cells, from the cell flags (one copy per plan)
+        std::vector<uint8_t> fl((size_t)c.N);
+        if (cudaMemcpy(fl.data(), c.flags, (size_t)c.N, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            delete p;
+            return CMF_ERR_CUDA;
+        }
+        std::vector<int> dam;
+        for (long i = 0; i < c.N; ++i)
+            if (fl[(size_t)i] & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM)) dam.push_back((int)i);
+        c.ND = (long)dam.size();
+        if (c.ND > 0) {
+            if (cudaMalloc(&p->dam_list, dam.size() * sizeof(int)) != cudaSuccess) {
+                delete p;
+                return CMF_ERR_CUDA;
+            }
+            if (cudaMemcpy(p->dam_list, dam.data(), dam.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+                cudaFree(p->dam_list);
+                delete p;
+                return CMF_ERR_CUDA;
+            }
+        }
+        c.dam = p->dam_list;
+    }
     c.grid_cells = (int)((c.N + kBlock - 1) / kBlock);
     c.grid_paths = (int)((c.P + kBlock - 1) / kBlock);
     p->grid = c.grid_cells;
@@ -1633,7 +1676,12 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
     return CMF_OK;
 }
 
-void cmf_adj_plan_destroy(CmfAdjPlan* plan) { delete plan; }
+void cmf_adj_plan_destroy(CmfAdjPlan* plan)
+{
+    if (!plan) return;
+    if (plan->dam_list) cudaFree(plan->dam_list);
+    delete plan;
+}
 
 int cmf_adj_sub_steps(CmfAdjPlan* plan, void* stream, const double* slot, double outer_seconds,
                       int* n_device)
@@ -1660,7 +1708,7 @@ int cmf_adj_forward(CmfAdjPlan* plan, void* stream, double* slots, int num_sub_s
         ka_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt);
         ka_stage<<<grid_all, kBlock, 0, s>>>(c, X, Y, runoff, dt);
         if (c.lev && c.NLV > 0)
-            ka_levee<<<(int)((c.NLV + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, Y);
+            ka_levee<<<(int)((c.NLV + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, Y);
     }
     return launch_status();
 }
@@ -1686,7 +1734,8 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         if (c.bif) kr_stage_path<<<c.grid_paths, kBlock, 0, s>>>(c, X, a);
         kr_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt, a);
         kr_momentum<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
-        if (c.res && c.R > 0) kr_dam<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        if (c.res && c.ND > 0)
+            kr_dam<<<(int)((c.ND * kDamDirs + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, runoff, dt, a);
         if (c.bif)
             kr_path<<<(int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, dt, a);
     }

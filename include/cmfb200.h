@@ -396,7 +396,9 @@ int cmf_forcing_apply(const CmfForcingMap* map, void* stream, const void* grid,
  *                   cross-section depth
  *   slot    a state's cell fields plus the sub-step's river/flood flux and
  *           limit rate ([15][N]), then the path state and the limited path
- *           fluxes ([3][P*L] + [2][P]); its length comes from cmf_adj_sizes
+ *           fluxes ([3][P*L] + [2][P]), then the flood-stage result of the
+ *           levee cells before their re-partition ([4][NLV]); its length
+ *           comes from cmf_adj_sizes
  *   lambda  adjoint of a state (state layout)
  *   grad    [4][N] river Manning, flood Manning, river height, river width
  *   scratch reverse-sweep intermediates; zero it before a sweep
@@ -404,8 +406,10 @@ int cmf_forcing_apply(const CmfForcingMap* map, void* stream, const void* grid,
  * The view must have CMF_FEAT_FP64 and one member (else
  * CMF_ERR_UNSUPPORTED).  The plan keeps the view's topology and parameter
  * pointers; the differentiated parameters are read through river_manning,
- * flood_manning, river_height and river_width.  All work is queued on
- * `stream`; nothing is allocated. */
+ * flood_manning, river_height and river_width.  cmf_adj_plan_create copies
+ * the cell flags to the host once to list the dam cells (a small device
+ * array owned by the plan); every other entry queues its work on `stream`
+ * and allocates nothing. */
 typedef struct CmfAdjPlan CmfAdjPlan;
 int cmf_adj_plan_create(const CmfView* view, CmfAdjPlan** out);
 void cmf_adj_plan_destroy(CmfAdjPlan* plan);
