@@ -29,9 +29,16 @@
 #include <cuda_runtime.h>
 #include "cmfb200.h"
 
-// minimum resident CTAs of k_stage per SM (caps its registers without spills)
+// minimum resident 256-thread CTAs per SM (register caps) of the sub-step kernels;
+// k_stage: 4 (64 registers, no spills)
 #ifndef CMF_STAGE_MIN_BLOCKS
 #define CMF_STAGE_MIN_BLOCKS 4
+#endif
+// k_momentum: 8 CTAs (32 registers) for one fp32 member, where the few bytes
+// it spills cost less than the occupancy they buy (182 -> 161 us per 6M
+// sub-step); fp64 and member-batched variants would spill hundreds of bytes
+#ifndef CMF_MOMENTUM_MIN_BLOCKS
+#define CMF_MOMENTUM_MIN_BLOCKS(REAL, ONE) ((sizeof(REAL) == 4 && (ONE)) ? 8 : 1)
 #endif
 
 namespace cmf {
@@ -485,7 +492,7 @@ __device__ __forceinline__ void momentum_path(const Dev<REAL>& v, long p, int m,
 }
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF>
-__global__ void __launch_bounds__(256) k_momentum(const Dev<REAL> v, int kh, int force_diag)
+__global__ void __launch_bounds__(256, CMF_MOMENTUM_MIN_BLOCKS(REAL, ONE)) k_momentum(const Dev<REAL> v, int kh, int force_diag)
 {
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
         long t = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
