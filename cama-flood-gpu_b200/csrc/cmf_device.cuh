@@ -108,6 +108,12 @@ struct Dev {
     // scratch fluxes
     REAL *qur, *quf;
     REAL* lrs;  // limit rate of the current sub-step, per cell x member
+    // Levee-indexed copies, packed once per plan (null where the plan keeps
+    // none): each levee cell's catchment area [NLV], floodplain row [NLV][K]
+    // and, when members share them, river height, width, length [3][NLV].
+    REAL* lpk_ca;
+    REAL* lpk_tbl;
+    REAL* lpk_geo;
 };
 
 // ---------------------------------------------------------------------------
@@ -697,7 +703,7 @@ template <typename REAL>
 __device__ __forceinline__ REAL clamp01(REAL x) { return fmin(fmax(x, (REAL)0), (REAL)1); }
 
 template <typename REAL, bool ONE>
-__device__ __forceinline__ void levee_stage(const Dev<REAL>& v, long ci, REAL l_crown,
+__device__ __forceinline__ void levee_stage(const Dev<REAL>& v, const REAL* row, REAL l_crown,
                                             REAL l_frac, REAL l_base_h, REAL ca, REAL rh,
                                             REAL rw, REAL rl, StageOut<REAL>& s, double& p_out,
                                             REAL& pdep_out)
@@ -729,7 +735,6 @@ __device__ __forceinline__ void levee_stage(const Dev<REAL>& v, long ci, REAL l_
          gradient_B = (REAL)0.0;
     bool found_B = false;
     bool scan_needed = true;
-    const REAL* row = v.tbl + ci * (long)nl;
     for (int l = 0; l < nl; ++l) {
         if (!scan_needed) break;
         REAL depth_val = row[l];
@@ -1010,6 +1015,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     v.rdep[im] = s.rdep;
     v.fdep[im] = s.fdep;
     v.ffr[im] = s.ffr;
+
     if (!lev_cell && st.diag) v.pdep[im] = s.fdep;
     if (res_cell) v.rti[im] = rti;
     if (st.diag) {
@@ -1100,19 +1106,35 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
             const long ci = v.lci[li];
             const long cm = ix<ONE>(ci, m, v.M);
             const REAL l_crown = v.lcrown[li], l_frac = v.lfrac[li], l_base = v.lbase[li];
-            const REAL rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, ci, m, v.M);
-            const REAL rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
-            const REAL rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
-            const REAL ca = v.ca[ci];
+            REAL rh, rw, rl, ca;
+            const REAL* row;
             StageOut<REAL> s;
             s.rs = rdst[cm];
             s.fs = fdst[cm];
             s.rdep = v.rdep[cm];
             s.fdep = v.fdep[cm];
             s.ffr = v.ffr[cm];
+            // static fields from the levee-indexed copies where the plan keeps
+            // them (coalesced over the levee list), else from the cells
+            if (v.lpk_ca) {
+                ca = v.lpk_ca[li];
+                row = v.lpk_tbl + li * (long)v.K;
+            } else {
+                ca = v.ca[ci];
+                row = v.tbl + ci * (long)v.K;
+            }
+            if (v.lpk_geo) {
+                rh = v.lpk_geo[li];
+                rw = v.lpk_geo[v.NLV + li];
+                rl = v.lpk_geo[2 * v.NLV + li];
+            } else {
+                rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, ci, m, v.M);
+                rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
+                rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
+            }
             double p_new;
             REAL pdep_new;
-            levee_stage<REAL, ONE>(v, ci, l_crown, l_frac, l_base, ca, rh, rw, rl, s, p_new,
+            levee_stage<REAL, ONE>(v, row, l_crown, l_frac, l_base, ca, rh, rw, rl, s, p_new,
                                    pdep_new);
             rdst[cm] = s.rs;
             fdst[cm] = s.fs;
@@ -1272,6 +1294,22 @@ __global__ void __launch_bounds__(256) k_copy_back(const Dev<REAL> v)
     if (t >= v.N * (long)v.M) return;
     v.rs0[t] = v.rs1[t];
     v.fs0[t] = v.fs1[t];
+}
+
+// Levee-indexed copies of the static fields k_levee reads (once per plan).
+template <typename REAL>
+__global__ void __launch_bounds__(256) k_levee_pack(const Dev<REAL> v)
+{
+    const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= v.NLV) return;
+    const long ci = v.lci[l];
+    v.lpk_ca[l] = v.ca[ci];
+    for (int k = 0; k < v.K; ++k) v.lpk_tbl[l * (long)v.K + k] = v.tbl[ci * (long)v.K + k];
+    if (v.lpk_geo) {
+        v.lpk_geo[l] = v.rh[ci];
+        v.lpk_geo[v.NLV + l] = v.rw[ci];
+        v.lpk_geo[2 * v.NLV + l] = v.rl[ci];
+    }
 }
 
 // Budget partials -> budget (fixed order), then clear partials.

@@ -91,7 +91,11 @@ KernelSet pick_one(bool one, bool res, bool lev, bool bif, bool bud)
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t qur, quf, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec, total;
+    size_t qur, quf, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec;
+    size_t base_total;  // the regions every caller needs
+    // levee-indexed copies that plans keep (after base_total; none without levees)
+    size_t lpk_ca, lpk_tbl, lpk_geo;
+    size_t total;
 };
 
 Layout layout_of(const CmfView* v, int cell_blocks)
@@ -111,6 +115,11 @@ Layout layout_of(const CmfView* v, int cell_blocks)
     L.bpart = o; o = align_up(o + (size_t)kBudgetTerms * (size_t)cell_blocks * 8);
     L.ctl = o; o = align_up(o + 16 * sizeof(int));
     L.tsec = o; o = align_up(o + 8);
+    L.base_total = o;
+    const size_t nlv = (v->features & CMF_FEAT_LEVEE) ? (size_t)v->num_levees : 0;
+    L.lpk_ca = o; o = align_up(o + nlv * real);
+    L.lpk_tbl = o; o = align_up(o + nlv * (size_t)v->num_flood_levels * real);
+    L.lpk_geo = o; o = align_up(o + 3 * nlv * real);
     L.total = o;
     return L;
 }
@@ -154,8 +163,10 @@ struct CmfPlan {
 
 namespace {
 
+// packed: bind the levee-indexed copies (plans); the allocation-free entry
+// leaves them null, and k_levee then reads the cell-indexed fields.
 template <typename REAL>
-void fill_dev(CmfPlan* p, const Layout& L)
+void fill_dev(CmfPlan* p, const Layout& L, bool packed)
 {
     const CmfView& v = p->view;
     Dev<REAL> d;
@@ -250,6 +261,12 @@ void fill_dev(CmfPlan* p, const Layout& L)
     d.qur = (REAL*)(ws + L.qur);
     d.quf = (REAL*)(ws + L.quf);
     d.lrs = (REAL*)(ws + L.lrs);
+    if (packed && d.NLV > 0) {
+        d.lpk_ca = (REAL*)(ws + L.lpk_ca);
+        d.lpk_tbl = (REAL*)(ws + L.lpk_tbl);
+        const int geo = CMF_BATCH_RIVER_HEIGHT | CMF_BATCH_RIVER_WIDTH | CMF_BATCH_RIVER_LENGTH;
+        if (!(v.batched_mask & geo)) d.lpk_geo = (REAL*)(ws + L.lpk_geo);
+    }
     std::memcpy(p->dev, &d, sizeof(d));
 }
 
@@ -597,16 +614,27 @@ int cmf_plan_create(const CmfView* view, CmfPlan** out)
     Layout L = layout_of(view, p->cell_blocks);
     if (p->fp64) {
         p->ks = pick_one<double>(p->one, res, lev, bif, bud);
-        fill_dev<double>(p, L);
+        fill_dev<double>(p, L, true);
     } else {
         p->ks = pick_one<float>(p->one, res, lev, bif, bud);
-        fill_dev<float>(p, L);
+        fill_dev<float>(p, L, true);
     }
     // clear the control words and budget partials once
     char* ws = (char*)view->workspace;
     if ((rc = check_cuda(cudaMemset(ws + L.bpart, 0, L.tsec + 8 - L.bpart))) != CMF_OK) {
         delete p;
         return rc;
+    }
+    if (p->levee_blocks > 0) {
+        // levee-indexed copies of the static fields k_levee reads
+        void* args[] = {p->dev};
+        const void* fn = p->fp64 ? (const void*)k_levee_pack<double> : (const void*)k_levee_pack<float>;
+        rc = launch(fn, ceil_div((long)view->num_levees, 256), 256, args, 0);
+        if (rc == CMF_OK) rc = check_cuda(cudaDeviceSynchronize());
+        if (rc != CMF_OK) {
+            delete p;
+            return rc;
+        }
     }
     *out = p;
     return CMF_OK;
@@ -907,8 +935,8 @@ extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
     v.workspace = scratch;
     v.workspace_bytes = kNoAllocScratchBytes;
     if ((rc = validate(&v)) != CMF_OK) return rc;
-    size_t need = 0;
-    if ((rc = cmf_workspace_size(&v, &need)) != CMF_OK) return rc;
+    // no levee-indexed copies here: only the regions every caller needs
+    const size_t need = layout_of(&v, ceil_div((long)v.num_catchments, block_of(&v))).base_total;
     if (need > kNoAllocScratchBytes) return CMF_ERR_ARG;
 
     // A plan on the stack: kernel set and device view, no graph.
@@ -927,10 +955,10 @@ extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
     Layout L = layout_of(&v, p.cell_blocks);
     if (p.fp64) {
         p.ks = pick_one<double>(true, res, lev, bif, bud);
-        fill_dev<double>(&p, L);
+        fill_dev<double>(&p, L, false);
     } else {
         p.ks = pick_one<float>(true, res, lev, bif, bud);
-        fill_dev<float>(&p, L);
+        fill_dev<float>(&p, L, false);
     }
     // The array keeps the previous call's contents: clear the control words
     // and the budget partials, which are accumulated rather than overwritten.
