@@ -266,12 +266,13 @@ def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: flo
 
 
 def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -> dict:
-    """The batched-ensemble workload at reduced size: `members` members of a
-    `basins`-basin network (~`catchments` catchments per member, runoff and
+    """The batched-ensemble workload: `members` members of a `basins`-basin
+    network (~`catchments` catchments per member, 6M by default; runoff and
     river Manning perturbed per member, daily forcing, per-member dt).  One
-    simulated day in a single member-innermost model (one launch per phase)
-    against the same members run one after another as plain models, both from
-    the same initial state on the same GPU."""
+    simulated day of the 30-day window (a bounded sample) in a single
+    member-innermost model (one launch per phase) against the same members run
+    one after another as plain models, both from the same initial state on the
+    same GPU."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn
     net = syn.generate_basins(basins, catchments, seed=3)
@@ -333,9 +334,10 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
     return {"value": batched, "looped_value": looped, "speedup": batched / looped,
             "unit": UNIT, "members": members, "catchments_per_member": n, "basins": basins,
             "sub_steps_per_member_mean": n_batched / members,
-            "workload": "1 day of a member-innermost ensemble (runoff x lognormal(0.3), "
-                        "river Manning x U(0.8,1.2) per member) vs the members looped as "
-                        "plain models; includes the state reset copies of the looped runs"}
+            "workload": "1 day (a sample of the 30-day window) of a member-innermost ensemble "
+                        "(runoff x lognormal(0.3), river Manning x U(0.8,1.2) per member) vs "
+                        "the members looped as plain models; includes the state reset copies "
+                        "of the looped runs"}
 
 
 def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
@@ -724,8 +726,9 @@ def main() -> None:
                     help="steps per chunk of the gridded-runoff forcing map leg (0 = skip)")
     ap.add_argument("--no-statistics", dest="statistics", action="store_false",
                     help="skip the output-statistics overhead leg")
-    ap.add_argument("--ensemble-catchments", type=int, default=600_000,
-                    help="catchments per member of that comparison (the full workload has ~6M)")
+    ap.add_argument("--ensemble-catchments", type=int, default=6_000_000,
+                    help="catchments per member of that comparison (the benchmark's ensemble "
+                         "workload: ~6M in 500 basins)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

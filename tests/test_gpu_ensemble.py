@@ -48,3 +48,42 @@ def test_batched_members_equal_plain_runs(members, device):
             np.testing.assert_array_equal(a[k][..., m].cpu().numpy(), b[k].cpu().numpy(),
                                           err_msg=f"member {m} field {k}")
     ens.check_status()
+
+
+@pytest.mark.parametrize("batched", [("river_manning",), ("river_height", "river_width")])
+def test_full_physics_members_equal_plain_runs(batched, device):
+    """Levees, bifurcation paths and reservoirs with per-member parameters:
+    member-batched river geometry makes the levee kernel read the cells'
+    geometry per member instead of the plan's levee-indexed copies."""
+    members = 4
+    net = syn.generate(syn.NetworkSpec(20_000, seed=19, bifurcation_paths=150, levee_fraction=0.25,
+                                       reservoirs=12))
+    n = net.num_catchments
+    rng = np.random.default_rng(19)
+    per = {k: (net.fields[k][:, None] * rng.uniform(0.85, 1.15, size=(n, members))).astype(np.float32)
+           for k in batched}
+    ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+                    num_members=members, batched_fields=per)
+    plains = []
+    for m in range(members):
+        f = dict(net.fields)
+        for k, v in per.items():
+            f[k] = np.ascontiguousarray(v[:, m])
+        plains.append(CaMaFlood(device=device, input_proxy=f, opened_modules=net.opened_modules))
+    order = ens.order
+    for day in range(2):
+        r = syn.daily_runoff(net, day)
+        ens.set_inputs(torch.as_tensor(np.repeat(r[order, None], members, axis=1)).to(device))
+        ens.step_advance()
+        for p in plains:
+            assert np.array_equal(p.order, order)
+            p.set_inputs(torch.as_tensor(r[order]).to(device))
+            p.step_advance()
+    torch.cuda.synchronize()
+    a = ens.state_tensors()
+    for m, p in enumerate(plains):
+        b = p.state_tensors()
+        for k in b:
+            np.testing.assert_array_equal(a[k][..., m].cpu().numpy(), b[k].cpu().numpy(),
+                                          err_msg=f"member {m} field {k}")
+    ens.check_status()
