@@ -55,6 +55,16 @@
 #include <cstring>
 #include <new>
 #include <vector>
+
+// Minimum resident 256-thread CTAs per SM of the long primal and reverse
+// kernels: 4 caps them at 64 registers.  They spill (kr_momentum most, ~0.4 KB
+// to L1), but the extra occupancy hides more gather latency: over a 3-day
+// window on the 250k full-physics network the reverse sub-step went from 299
+// to 242 us and the forward from 70 to 67 us.  5 CTAs (48 registers) slowed
+// both.
+#ifndef CMF_ADJ_MIN_BLOCKS
+#define CMF_ADJ_MIN_BLOCKS 4
+#endif
 #include <cuda_runtime.h>
 
 namespace {
@@ -809,7 +819,7 @@ __device__ __forceinline__ double store_eval(double rsto, double fsto, double pr
 // ---------------------------------------------------------------------------
 // forward kernels (tape)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) ka_momentum(const Ctx c, double* X, double* Y,
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) ka_momentum(const Ctx c, double* X, double* Y,
                                                       const double* runoff, double dt)
 {
     if ((int)blockIdx.x >= c.grid_cells) {
@@ -914,7 +924,7 @@ __global__ void __launch_bounds__(kBlock) ka_stage(const Ctx c, const double* X,
 
 // Levee re-partition of the levee cells (levee.cu:29-261) on the flood-stage
 // result ka_stage left in Y, over the compact levee list.
-__global__ void __launch_bounds__(kBlock) ka_levee(const Ctx c, double* X, double* Y)
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) ka_levee(const Ctx c, double* X, double* Y)
 {
     const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= c.NLV) return;
@@ -1038,7 +1048,7 @@ __global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const doubl
     q[9] = lam[F_PDEP * N + i];
 }
 
-__global__ void __launch_bounds__(kBlock) kr_levee(const Ctx c, Adj a)
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx c, Adj a)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.NLV * 6L) return;
@@ -1057,7 +1067,7 @@ __global__ void __launch_bounds__(kBlock) kr_levee(const Ctx c, Adj a)
 }
 
 // Stage, levee and storage update reversed (kr_stage).
-__global__ void __launch_bounds__(kBlock) kr_stage(const Ctx c, const double* X,
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_stage(const Ctx c, const double* X,
                                                    const double* runoff, double dt, Adj a)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1251,7 +1261,7 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
 // (6 end-state inputs and two per level) evaluates one dual pass of the path
 // flux and writes that input's adjoint: lambda_k of the path state, or an
 // end-state adjoint left for the end cell.
-__global__ void __launch_bounds__(kBlock) kr_path(const Ctx c, const double* X, double dt, Adj a)
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_path(const Ctx c, const double* X, double dt, Adj a)
 {
     const int L = c.L;
     const int NI = 6 + 2 * L;
@@ -1302,7 +1312,7 @@ __global__ void __launch_bounds__(kBlock) kr_path(const Ctx c, const double* X, 
 
 // Momentum reversed (kr_momentum): lambda_k of the cell, the downstream-depth
 // adjoint left for the downstream cell, parameter gradients.
-__global__ void __launch_bounds__(kBlock) kr_momentum(const Ctx c, const double* X,
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const Ctx c, const double* X,
                                                       const double* runoff, double dt, Adj a)
 {
     const long N = c.N;
