@@ -33,7 +33,7 @@
 //   kr_dam         reservoir release and the dam-upstream kinematic flow
 //                  reversed for the dam cells;
 //   kr_path        path momentum reversed, one thread per path and input
-//                  direction.
+//                  direction (trailing blocks of the kr_momentum launch).
 //
 // The long scalar branches -- reservoir release, dam-upstream kinematic flow,
 // path momentum with its limiter, levee re-partition -- are templates on the
@@ -1261,11 +1261,16 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
 // (6 end-state inputs and two per level) evaluates one dual pass of the path
 // flux and writes that input's adjoint: lambda_k of the path state, or an
 // end-state adjoint left for the end cell.
-__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_path(const Ctx c, const double* X, double dt, Adj a)
+// Path momentum reversed, direction thread t (p = t / (6 + 2L)).  Runs as the
+// trailing blocks of the kr_momentum launch: it reads the tape, the
+// outgoing-storage adjoint of kr_limit and the path buffers of kr_stage_path,
+// and writes only the path lambdas and the path-end buffer, none of which the
+// momentum or dam reverse touches.
+__device__ __forceinline__ void path_reverse(const Ctx& c, const double* X, double dt, const Adj& a,
+                                             long t)
 {
     const int L = c.L;
     const int NI = 6 + 2 * L;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.P * (long)NI) return;
     const long p = t / NI;
     const int j = (int)(t - p * NI);
@@ -1315,6 +1320,10 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_path(const Ctx 
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const Ctx c, const double* X,
                                                       const double* runoff, double dt, Adj a)
 {
+    if ((int)blockIdx.x >= c.grid_cells) {
+        path_reverse(c, X, dt, a, (long)(blockIdx.x - c.grid_cells) * blockDim.x + threadIdx.x);
+        return;
+    }
     const long N = c.N;
     double* lam = a.lam;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1743,11 +1752,11 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         kr_stage<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
         if (c.bif) kr_stage_path<<<c.grid_paths, kBlock, 0, s>>>(c, X, a);
         kr_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt, a);
-        kr_momentum<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        // cells, then (with paths) the path direction threads in trailing blocks
+        const int path_blocks = c.bif ? (int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock) : 0;
+        kr_momentum<<<c.grid_cells + path_blocks, kBlock, 0, s>>>(c, X, runoff, dt, a);
         if (c.res && c.ND > 0)
             kr_dam<<<(int)((c.ND * kDamDirs + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, runoff, dt, a);
-        if (c.bif)
-            kr_path<<<(int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, dt, a);
     }
     return launch_status();
 }
