@@ -65,6 +65,27 @@
 #ifndef CMF_ADJ_MIN_BLOCKS
 #define CMF_ADJ_MIN_BLOCKS 4
 #endif
+
+// Programmatic dependent launch, for the reverse sweep (the forward chain
+// measured slower with it: 67 -> 69.6 us per sub-step, against 236 -> 223 us
+// for the reverse).  The sweep is a chain of dependent, latency-bound
+// launches whose last wave is partly empty.  Each kernel lets
+// the next one launch as soon as all of its own blocks are resident, so the
+// next grid's blocks are scheduled during this one's tail; they then wait in
+// hardware until this grid has completed and its writes are visible.  The
+// dependents launch only after every block of the running grid has started,
+// so they never hold back its blocks.  Kernels launched without the
+// attribute (or after a kernel that does not trigger) just start after it.
+#ifndef CMF_ADJ_PDL
+#define CMF_ADJ_PDL 1
+#endif
+__device__ __forceinline__ void pdl_begin()
+{
+#if CMF_ADJ_PDL
+    cudaTriggerProgrammaticLaunchCompletion();
+    cudaGridDependencySynchronize();
+#endif
+}
 #include <cuda_runtime.h>
 
 namespace {
@@ -1027,6 +1048,7 @@ __device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a
 __global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const double* X,
                                                         const double* runoff, double dt, Adj a)
 {
+    pdl_begin();
     const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= c.NLV) return;
     const long N = c.N;
@@ -1050,6 +1072,7 @@ __global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const doubl
 
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx c, Adj a)
 {
+    pdl_begin();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.NLV * 6L) return;
     const long l = t / 6;
@@ -1070,6 +1093,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_stage(const Ctx c, const double* X,
                                                    const double* runoff, double dt, Adj a)
 {
+    pdl_begin();
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
     const long N = c.N;
@@ -1147,6 +1171,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_stage(const Ctx
 // limit-rate scaling of the level fluxes.
 __global__ void __launch_bounds__(kBlock) kr_stage_path(const Ctx c, const double* X, Adj a)
 {
+    pdl_begin();
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= c.P) return;
     const long N = c.N;
@@ -1196,6 +1221,7 @@ __global__ void __launch_bounds__(kBlock) kr_stage_path(const Ctx c, const doubl
 // terms of its bifurcation ends.
 __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X, double dt, Adj a)
 {
+    pdl_begin();
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= c.N) return;
     const long N = c.N;
@@ -1320,6 +1346,7 @@ __device__ __forceinline__ void path_reverse(const Ctx& c, const double* X, doub
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const Ctx c, const double* X,
                                                       const double* runoff, double dt, Adj a)
 {
+    pdl_begin();
     if ((int)blockIdx.x >= c.grid_cells) {
         path_reverse(c, X, dt, a, (long)(blockIdx.x - c.grid_cells) * blockDim.x + threadIdx.x);
         return;
@@ -1488,6 +1515,7 @@ constexpr int kDamDirs = 7;
 __global__ void __launch_bounds__(kBlock) kr_dam(const Ctx c, const double* X,
                                                  const double* runoff, double dt, Adj a)
 {
+    pdl_begin();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.ND * (long)kDamDirs) return;
     const long d = t / kDamDirs;
@@ -1537,6 +1565,25 @@ __global__ void __launch_bounds__(kBlock) kr_finalize(const Ctx c, Adj a)
     apply_pending(c, i, a);
 }
 
+}  // namespace
+
+namespace {
+template <typename... KArgs, typename... Args>
+void launch_dep(void (*kernel)(KArgs...), int grid, cudaStream_t s, Args... args)
+{
+    if (grid <= 0) return;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = CMF_ADJ_PDL;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 }  // namespace
 
 struct CmfAdjPlan {
@@ -1746,17 +1793,17 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
     for (int k = num_sub_steps - 1; k >= 0; --k) {
         const double* X = tape + (long)k * stride;
         if (c.lev && c.NLV > 0) {
-            kr_levee_prep<<<(int)((c.NLV + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, runoff, dt, a);
-            kr_levee<<<(int)((c.NLV * 6 + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, a);
+            launch_dep(kr_levee_prep, (int)((c.NLV + kBlock - 1) / kBlock), s, c, X, runoff, dt, a);
+            launch_dep(kr_levee, (int)((c.NLV * 6 + kBlock - 1) / kBlock), s, c, a);
         }
-        kr_stage<<<c.grid_cells, kBlock, 0, s>>>(c, X, runoff, dt, a);
-        if (c.bif) kr_stage_path<<<c.grid_paths, kBlock, 0, s>>>(c, X, a);
-        kr_limit<<<c.grid_cells, kBlock, 0, s>>>(c, X, dt, a);
+        launch_dep(kr_stage, c.grid_cells, s, c, X, runoff, dt, a);
+        if (c.bif) launch_dep(kr_stage_path, c.grid_paths, s, c, X, a);
+        launch_dep(kr_limit, c.grid_cells, s, c, X, dt, a);
         // cells, then (with paths) the path direction threads in trailing blocks
         const int path_blocks = c.bif ? (int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock) : 0;
-        kr_momentum<<<c.grid_cells + path_blocks, kBlock, 0, s>>>(c, X, runoff, dt, a);
+        launch_dep(kr_momentum, c.grid_cells + path_blocks, s, c, X, runoff, dt, a);
         if (c.res && c.ND > 0)
-            kr_dam<<<(int)((c.ND * kDamDirs + kBlock - 1) / kBlock), kBlock, 0, s>>>(c, X, runoff, dt, a);
+            launch_dep(kr_dam, (int)((c.ND * kDamDirs + kBlock - 1) / kBlock), s, c, X, runoff, dt, a);
     }
     return launch_status();
 }
