@@ -340,11 +340,20 @@ __device__ __forceinline__ void path_flux(const Ctx& c, long p, const T* in, dou
 }
 
 // Levee re-partition (levee.cu:29-261) of a levee cell after its flood stage.
-// in = (river storage, flood storage, river depth, flood depth, river width,
-// river height); out = (river, flood, protected storage, river, flood,
-// protected depth); the flooded fraction passes through `ffr` (value only).
+// in = (river storage, flood storage, river depth, flood depth), geometry =
+// (river width, river height); out = (river, flood, protected storage, river,
+// flood, protected depth); the flooded fraction passes through `ffr` (value
+// only).  T is the scalar of everything the state reaches, G that of what
+// depends on the geometry alone (the floodplain scan): a reverse pass along a
+// state direction runs the scan on plain doubles.
 template <typename T>
-__device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, double& ffr, T* out)
+__device__ __forceinline__ T up(double x) { return cnst<T>(x); }
+template <typename T>
+__device__ __forceinline__ T up(const Dual& x) { return x; }
+
+template <typename T, typename G>
+__device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, G rw, G rh,
+                                           double& ffr, T* out)
 {
     const int slot = c.lslot[ci];
     const int nl = c.K;
@@ -352,8 +361,8 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
     const double l_crown = c.lcrown[slot], l_frac = c.lfrac[slot], l_base_h = c.lbase[slot];
     const T riv_sto_curr = in[0], fld_sto_curr = in[1];
     const T total_sto = riv_sto_curr + fld_sto_curr;
-    const T r_dep_curr = in[2], fld_depth_curr = in[3], rw = in[4], rh = in[5];
-    T riv_max_sto = rl * rw * rh;
+    const T r_dep_curr = in[2], fld_depth_curr = in[3];
+    G riv_max_sto = rl * rw * rh;
     if (!(val(total_sto) >= val(riv_max_sto))) {
         out[0] = riv_sto_curr;
         out[1] = fld_sto_curr;
@@ -365,14 +374,14 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
     }
     const double dwth_inc = (ca / rl) / (double)nl;
     const double levee_dist = l_frac * (ca / rl);
-    T s_curr = riv_max_sto;
+    G s_curr = riv_max_sto;
     double dhgt_pre = 0.0;
-    T dwth_pre = rw;
-    T levee_base_sto = riv_max_sto;
-    T levee_fill_sto = riv_max_sto;
+    G dwth_pre = rw;
+    G levee_base_sto = riv_max_sto;
+    G levee_fill_sto = riv_max_sto;
     bool found_base = false, found_fill = false;
     const int ilev = (int)(l_frac * (double)nl);
-    T dsto_fil_B = cnst<T>(0.0), dwth_fil_B = cnst<T>(0.0);
+    G dsto_fil_B = cnst<G>(0.0), dwth_fil_B = cnst<G>(0.0);
     double ddph_fil_B = 0.0, gradient_B = 0.0;
     bool found_B = false;
     bool scan_needed = true;
@@ -381,34 +390,34 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
         if (!scan_needed) break;
         const double depth_val = row[l];
         const double dhgt_seg = fmax(depth_val - dhgt_pre, 1e-6);
-        T dwth_mid = dwth_pre + 0.5 * dwth_inc;
-        T dsto_seg = rl * dwth_mid * dhgt_seg;
-        T s_next = s_curr + dsto_seg;
+        G dwth_mid = dwth_pre + 0.5 * dwth_inc;
+        G dsto_seg = rl * dwth_mid * dhgt_seg;
+        G s_next = s_curr + dsto_seg;
         const double gradient = dhgt_seg / dwth_inc;
 
         const bool cond_base = (l_base_h > dhgt_pre) && (l_base_h <= depth_val);
         const double ratio_base = (l_base_h - dhgt_pre) / dhgt_seg;
-        T dsto_base_p = rl * (dwth_pre + 0.5 * ratio_base * dwth_inc) * (ratio_base * dhgt_seg);
+        G dsto_base_p = rl * (dwth_pre + 0.5 * ratio_base * dwth_inc) * (ratio_base * dhgt_seg);
         if (cond_base && !found_base) levee_base_sto = s_curr + dsto_base_p;
         found_base = found_base || cond_base;
 
         const bool cond_fill = (l_crown > dhgt_pre) && (l_crown <= depth_val);
         const double ratio_fill = (l_crown - dhgt_pre) / dhgt_seg;
-        T dsto_fill_p = rl * (dwth_pre + 0.5 * ratio_fill * dwth_inc) * (ratio_fill * dhgt_seg);
+        G dsto_fill_p = rl * (dwth_pre + 0.5 * ratio_fill * dwth_inc) * (ratio_fill * dhgt_seg);
         if (cond_fill && !found_fill) levee_fill_sto = s_curr + dsto_fill_p;
         found_fill = found_fill || cond_fill;
 
         const double dhgt_dif_loop = l_crown - l_base_h;
-        T s_top_loop = levee_base_sto + (levee_dist + rw) * dhgt_dif_loop * rl;
-        T dsto_add_wedge = (levee_dist + rw) * (l_crown - depth_val) * rl;
-        T threshold = s_next + dsto_add_wedge;
+        G s_top_loop = levee_base_sto + (levee_dist + rw) * dhgt_dif_loop * rl;
+        G dsto_add_wedge = (levee_dist + rw) * (l_crown - depth_val) * rl;
+        G threshold = s_next + dsto_add_wedge;
 
         const bool cond_check = (l >= ilev) && !found_B;
         const bool cond_found = cond_check && (val(total_sto) < val(threshold));
-        T current_lb = (l == ilev) ? s_top_loop : dsto_fil_B;
+        G current_lb = (l == ilev) ? s_top_loop : dsto_fil_B;
         if (cond_check && !cond_found) {
             dsto_fil_B = threshold;
-            dwth_fil_B = cnst<T>(dwth_inc * (double)(l + 1) - levee_dist);
+            dwth_fil_B = cnst<G>(dwth_inc * (double)(l + 1) - levee_dist);
             ddph_fil_B = depth_val - l_base_h;
         } else {
             dsto_fil_B = current_lb;
@@ -421,19 +430,19 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
         dwth_pre = dwth_pre + dwth_inc;
         scan_needed = !(found_base && found_fill && found_B);
     }
-    T s_base_extra = s_curr + rl * dwth_pre * (l_base_h - dhgt_pre);
+    G s_base_extra = s_curr + rl * dwth_pre * (l_base_h - dhgt_pre);
     if (!found_base) levee_base_sto = (l_base_h > dhgt_pre) ? s_base_extra : riv_max_sto;
-    T s_fill_extra = s_curr + rl * dwth_pre * (l_crown - dhgt_pre);
+    G s_fill_extra = s_curr + rl * dwth_pre * (l_crown - dhgt_pre);
     if (!found_fill) levee_fill_sto = (l_crown > dhgt_pre) ? s_fill_extra : riv_max_sto;
 
     const double dhgt_dif = l_crown - l_base_h;
-    T s_top = levee_base_sto + (levee_dist + rw) * dhgt_dif * rl;
+    G s_top = levee_base_sto + (levee_dist + rw) * dhgt_dif * rl;
     const bool is_case4 = val(total_sto) >= val(levee_fill_sto);
     const bool is_case3 = (!is_case4) && (val(total_sto) >= val(s_top));
     const bool is_case2 = (!is_case4) && (!is_case3) && (val(total_sto) >= val(levee_base_sto));
 
     T dsto_add_c2 = total_sto - levee_base_sto;
-    T dwth_add_c2 = levee_dist + rw;
+    G dwth_add_c2 = levee_dist + rw;
     T f_dph_c2 = l_base_h + dsto_add_c2 / dwth_add_c2 / rl;
     T r_sto_c2 = riv_max_sto + rl * rw * f_dph_c2;
     T r_dph_c2 = r_sto_c2 / rl / rw;
@@ -451,17 +460,17 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
     T p_dph_B = found_B ? p_dph_B_found : p_dph_B_extra;
     const double f_frc_B = found_B ? f_frc_B_found : 1.0;
 
-    T r_sto_c3 = riv_max_sto + rl * rw * l_crown;
-    T r_dph_c3 = r_sto_c3 / rl / rw;
-    T f_sto_c3 = vmax(s_top - r_sto_c3, cnst<T>(0.0));
+    G r_sto_c3 = riv_max_sto + rl * rw * l_crown;
+    G r_dph_c3 = r_sto_c3 / rl / rw;
+    G f_sto_c3 = vmax(s_top - r_sto_c3, cnst<G>(0.0));
     const double f_frc_c3 = fmin(fmax(f_frc_B, 0.0), 1.0);
 
     T f_dph_c4 = fld_depth_curr;
     T dsto_add_c4 = (f_dph_c4 - l_crown) * (levee_dist + rw) * rl;
     T f_sto_c4 = vmax(s_top + dsto_add_c4 - riv_sto_curr, cnst<T>(0.0));
 
-    T r_sto_candidate = is_case2 ? r_sto_c2 : (is_case3 ? r_sto_c3 : riv_sto_curr);
-    T f_sto_candidate = is_case2 ? f_sto_c2 : (is_case3 ? f_sto_c3 : (is_case4 ? f_sto_c4 : fld_sto_curr));
+    T r_sto_candidate = is_case2 ? r_sto_c2 : (is_case3 ? up<T>(r_sto_c3) : riv_sto_curr);
+    T f_sto_candidate = is_case2 ? f_sto_c2 : (is_case3 ? up<T>(f_sto_c3) : (is_case4 ? f_sto_c4 : fld_sto_curr));
     const bool no_levee_partition = !is_case2 && !is_case3 && !is_case4;
     T r_sto = (is_case4 || no_levee_partition) ? riv_sto_curr : vmin(r_sto_candidate, total_sto);
     T remaining_sto = total_sto - r_sto;
@@ -474,7 +483,7 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, d
     out[0] = r_sto;
     out[1] = f_sto;
     out[2] = p_sto;
-    out[3] = is_case2 ? r_dph_c2 : (is_case3 ? r_dph_c3 : r_dep_curr);
+    out[3] = is_case2 ? r_dph_c2 : (is_case3 ? up<T>(r_dph_c3) : r_dep_curr);
     out[4] = is_case2 ? f_dph_c2 : (is_case3 ? cnst<T>(l_crown) : fld_depth_curr);
     out[5] = is_case2 ? cnst<T>(0.0) : (is_case3 ? p_dph_B : (is_case4 ? f_dph_c4 : cnst<T>(0.0)));
     ffr = is_case2 ? f_frc_c2 : (is_case3 ? f_frc_c3 : ffr);
@@ -957,7 +966,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) ka_levee(const Ctx
 #pragma unroll
     for (int k = 0; k < 4; ++k) rec[k * c.NLV + l] = in[k];
     double out[6], ffr = 0.0;
-    levee_part<double>(c, i, in, ffr, out);
+    levee_part<double, double>(c, i, in, in[4], in[5], ffr, out);
     Y[F_RS * N + i] = out[0];
     Y[F_FS * N + i] = out[1];
     Y[F_PS * N + i] = out[2];
@@ -1073,17 +1082,33 @@ __global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const doubl
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx c, Adj a)
 {
     pdl_begin();
+    // threads [0, 4 NLV): the four state directions of each levee; then
+    // [4 NLV, 6 NLV): the two geometry directions -- so that a warp runs one
+    // instantiation of levee_part
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= c.NLV * 6L) return;
-    const long l = t / 6;
-    const int j = (int)(t - l * 6);
+    const long nlv = c.NLV;
+    if (t >= nlv * 6L) return;
+    long l;
+    int j;
+    if (t < 4 * nlv) {
+        l = t >> 2;
+        j = (int)(t & 3);
+    } else {
+        const long u = t - 4 * nlv;
+        l = u >> 1;
+        j = 4 + (int)(u & 1);
+    }
     const long i = c.lci[l];
     const double* q = levin(c, a.scr) + 10 * l;
-    const double in[6] = {q[0], q[1], q[2], q[3], c.rw[i], c.rh[i]};
-    Dual x[6], y[6];
-    for (int k = 0; k < 6; ++k) x[k] = {in[k], k == j ? 1.0 : 0.0};
+    Dual x[4], y[6];
+    for (int k = 0; k < 4; ++k) x[k] = {q[k], k == j ? 1.0 : 0.0};
     double ffr = 0.0;
-    levee_part<Dual>(c, i, x, ffr, y);
+    if (j < 4) {
+        levee_part<Dual, double>(c, i, x, c.rw[i], c.rh[i], ffr, y);
+    } else {
+        const Dual rw = {c.rw[i], j == 4 ? 1.0 : 0.0}, rh = {c.rh[i], j == 5 ? 1.0 : 0.0};
+        levee_part<Dual, Dual>(c, i, x, rw, rh, ffr, y);
+    }
     double v = 0.0;
     for (int o = 0; o < 6; ++o) v += q[4 + o] * y[o].d;
     levb(c, a.scr)[6 * l + j] = v;
