@@ -31,7 +31,8 @@
 //   kr_limit       limit-rate and outgoing-storage adjoints;
 //   kr_momentum    local-inertial momentum reversed per cell;
 //   kr_dam         reservoir release and the dam-upstream kinematic flow
-//                  reversed for the dam cells;
+//                  reversed for the dam cells (trailing blocks of the
+//                  kr_momentum launch, applied one sub-step later);
 //   kr_path        path momentum reversed, one thread per path and input
 //                  direction (trailing blocks of the kr_momentum launch).
 //
@@ -106,6 +107,7 @@ enum Grad { G_RMAN = 0, G_FMAN, G_RH, G_RW, kGradFields };
 
 constexpr int kBlock = 256;
 constexpr int kMaxLevels = 8;
+constexpr int kDamDirs = 7;  // input directions of the dam-upstream kinematic flow
 constexpr int kMaxFloodLevels = 16;
 constexpr double kFloor = 1e-6;
 constexpr double kFloor2 = 1e-6 * 1e-6;
@@ -198,9 +200,11 @@ struct Ctx {
     // bifurcation
     const int *bptr, *bpaths, *bci, *bdi;
     const double *bman, *bwid, *blen, *belv;
-    // dam cells (reservoir or dam-upstream), compact
+    // dam cells (reservoir or dam-upstream), compact, and each cell's index
+    // in that list (-1 elsewhere)
     long ND;
     const int* dam;
+    const int* dam_slot;
     // slot geometry (doubles); lev_off: the pre-levee stage of the levee
     // cells [4][NLV] (river/flood storage, river/flood depth) that ka_levee
     // records in the slot of its sub-step for kr_levee_prep
@@ -1016,6 +1020,8 @@ __device__ __forceinline__ double* bcsdb(const Ctx& c, double* scr) { return psc
 __device__ __forceinline__ double* peb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P + 2 * c.P * c.L; }
 __device__ __forceinline__ double* levb(const Ctx& c, double* scr) { return peb(c, scr) + 8 * c.P; }
 __device__ __forceinline__ double* levin(const Ctx& c, double* scr) { return levb(c, scr) + 6 * c.NLV; }
+// dam scratch: the deferred dam adjoints, DAMB [ND][kDamDirs]
+__device__ __forceinline__ double* damb(const Ctx& c, double* scr) { return levin(c, scr) + 10 * c.NLV; }
 
 // Apply the adjoints the later sub-step's momentum (downstream depth) and path
 // kernels (end states) left for cell i; returns nothing, updates lam / grad.
@@ -1040,6 +1046,23 @@ __device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a
     }
     lam[F_RDEP * N + i] += rdep_bar;
     a.grad[G_RH * N + i] -= rdep_bar;
+    if (c.ND > 0 && (fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) {
+        // what the later sub-step's dam reverse left for this cell
+        const double* db = damb(c, a.scr) + (long)kDamDirs * c.dam_slot[i];
+        if (fl & CMF_CELL_RESERVOIR) {
+            lam[F_RS * N + i] += db[0];
+            lam[F_FS * N + i] += db[1];
+            lam[F_RTI * N + i] += db[2];
+        } else {
+            lam[F_RDEP * N + i] += db[0];
+            lam[F_FDEP * N + i] += db[1];
+            lam[F_RS * N + i] += db[2];
+            lam[F_FS * N + i] += db[3];
+            a.grad[G_RW * N + i] += db[4];
+            a.grad[G_RMAN * N + i] += db[5];
+            a.grad[G_FMAN * N + i] += db[6];
+        }
+    }
     if (pdep_bar != 0.0) lam[F_PDEP * N + i] += pdep_bar;
     if (tot_bar != 0.0) {
         lam[F_RS * N + i] += tot_bar;
@@ -1368,12 +1391,19 @@ __device__ __forceinline__ void path_reverse(const Ctx& c, const double* X, doub
 
 // Momentum reversed (kr_momentum): lambda_k of the cell, the downstream-depth
 // adjoint left for the downstream cell, parameter gradients.
+__device__ __forceinline__ void dam_reverse(const Ctx& c, const double* X, const double* runoff,
+                                            double dt, const Adj& a, long t);
+
 __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const Ctx c, const double* X,
                                                       const double* runoff, double dt, Adj a)
 {
     pdl_begin();
     if ((int)blockIdx.x >= c.grid_cells) {
-        path_reverse(c, X, dt, a, (long)(blockIdx.x - c.grid_cells) * blockDim.x + threadIdx.x);
+        // trailing blocks: path direction threads, then dam direction threads
+        const long b = (long)blockIdx.x - c.grid_cells;
+        const long pb = c.bif ? (c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock : 0;
+        if (b < pb) path_reverse(c, X, dt, a, b * blockDim.x + threadIdx.x);
+        else dam_reverse(c, X, runoff, dt, a, (b - pb) * blockDim.x + threadIdx.x);
         return;
     }
     const long N = c.N;
@@ -1532,25 +1562,24 @@ __device__ __forceinline__ void flux_bars(const Ctx& c, const double* X, const A
 }
 
 // Reservoir release and dam-upstream kinematic flow reversed (kr_dam), one
-// thread per dam cell and input direction (one dual pass each; the
-// directions of a cell write distinct fields), after kr_momentum: it adds to
-// what kr_momentum wrote.
-constexpr int kDamDirs = 7;
-
-__global__ void __launch_bounds__(kBlock) kr_dam(const Ctx c, const double* X,
-                                                 const double* runoff, double dt, Adj a)
+// thread per dam cell and input direction (one dual pass each), as trailing
+// blocks of the kr_momentum launch.  kr_momentum writes the same cells'
+// lambdas, so these adjoints go to the dam scratch instead and apply_pending
+// adds them at the start of the earlier sub-step (before anything reads those
+// lambdas); the runoff gradient, which kr_momentum never writes and which
+// belongs to this sub-step's interval, is added at once.
+__device__ __forceinline__ void dam_reverse(const Ctx& c, const double* X, const double* runoff,
+                                            double dt, const Adj& a, long t)
 {
-    pdl_begin();
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.ND * (long)kDamDirs) return;
     const long d = t / kDamDirs;
     const int j = (int)(t - d * kDamDirs);
     const long i = c.dam[d];
     const uint8_t fl = c.flags[i];
     const long N = c.N;
-    double* lam = a.lam;
     double qr_bar, qf_bar;
     flux_bars(c, X, a, i, dt, qr_bar, qf_bar);
+    double* db = damb(c, a.scr) + (long)kDamDirs * d;
     if (fl & CMF_CELL_RESERVOIR) {
         if (j >= 4) return;
         const double in[4] = {X[F_RS * N + i], X[F_FS * N + i], X[F_RTI * N + i], runoff[i]};
@@ -1559,26 +1588,15 @@ __global__ void __launch_bounds__(kBlock) kr_dam(const Ctx c, const double* X,
         const double ib = 0.0 + vjp_column<4, 1>(in, ob, j, [&](const Dual* x, Dual* y) {
             y[0] = release<Dual>(c, slot, x[0], x[1], x[2], x[3], dt);
         });
-        double* dst = j == 0 ? lam + F_RS * N : j == 1 ? lam + F_FS * N : j == 2 ? lam + F_RTI * N : a.groff;
-        dst[i] += ib;
+        if (j == 3) a.groff[i] += ib;
+        else db[j] = ib;
     } else {
         const double in[7] = {X[F_RDEP * N + i], X[F_FDEP * N + i], X[F_RS * N + i],
                               X[F_FS * N + i], c.rw[i], c.rman[i], c.fman[i]};
         const double ob[2] = {qr_bar, qf_bar};
-        const double ib = 0.0 + vjp_column<7, 2>(in, ob, j, [&](const Dual* x, Dual* y) {
+        db[j] = 0.0 + vjp_column<7, 2>(in, ob, j, [&](const Dual* x, Dual* y) {
             kinematic<Dual>(c, i, x[0], x[1], x[2], x[3], x[4], x[5], x[6], dt, y[0], y[1]);
         });
-        double* dst;
-        switch (j) {
-        case 0: dst = lam + F_RDEP * N; break;
-        case 1: dst = lam + F_FDEP * N; break;
-        case 2: dst = lam + F_RS * N; break;
-        case 3: dst = lam + F_FS * N; break;
-        case 4: dst = a.grad + G_RW * N; break;
-        case 5: dst = a.grad + G_RMAN * N; break;
-        default: dst = a.grad + G_FMAN * N; break;
-        }
-        dst[i] += ib;
     }
 }
 
@@ -1615,6 +1633,7 @@ struct CmfAdjPlan {
     Ctx ctx;
     int grid;
     int* dam_list;  // device, ctx.ND entries
+    int* dam_slot;  // device, N entries
 };
 
 namespace {
@@ -1626,7 +1645,7 @@ int launch_status()
 
 long scratch_len(const Ctx& c)
 {
-    return (long)kCellScratch * c.N + 2 * c.P + 2 * c.P * c.L + 8 * c.P + 16 * c.NLV;
+    return (long)kCellScratch * c.N + 2 * c.P + 2 * c.P * c.L + 8 * c.P + 16 * c.NLV + kDamDirs * c.ND;
 }
 
 }  // namespace
@@ -1747,18 +1766,23 @@ int cmf_adj_plan_create(const CmfView* v, CmfAdjPlan** out)
             if (fl[(size_t)i] & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM)) dam.push_back((int)i);
         c.ND = (long)dam.size();
         if (c.ND > 0) {
-            if (cudaMalloc(&p->dam_list, dam.size() * sizeof(int)) != cudaSuccess) {
-                delete p;
-                return CMF_ERR_CUDA;
-            }
-            if (cudaMemcpy(p->dam_list, dam.data(), dam.size() * sizeof(int), cudaMemcpyHostToDevice) !=
-                cudaSuccess) {
-                cudaFree(p->dam_list);
+            std::vector<int> slot((size_t)c.N, -1);
+            for (size_t d = 0; d < dam.size(); ++d) slot[(size_t)dam[d]] = (int)d;
+            bool ok = cudaMalloc(&p->dam_list, dam.size() * sizeof(int)) == cudaSuccess &&
+                      cudaMalloc(&p->dam_slot, slot.size() * sizeof(int)) == cudaSuccess &&
+                      cudaMemcpy(p->dam_list, dam.data(), dam.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice) == cudaSuccess &&
+                      cudaMemcpy(p->dam_slot, slot.data(), slot.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice) == cudaSuccess;
+            if (!ok) {
+                if (p->dam_list) cudaFree(p->dam_list);
+                if (p->dam_slot) cudaFree(p->dam_slot);
                 delete p;
                 return CMF_ERR_CUDA;
             }
         }
         c.dam = p->dam_list;
+        c.dam_slot = p->dam_slot;
     }
     c.grid_cells = (int)((c.N + kBlock - 1) / kBlock);
     c.grid_paths = (int)((c.P + kBlock - 1) / kBlock);
@@ -1771,6 +1795,7 @@ void cmf_adj_plan_destroy(CmfAdjPlan* plan)
 {
     if (!plan) return;
     if (plan->dam_list) cudaFree(plan->dam_list);
+    if (plan->dam_slot) cudaFree(plan->dam_slot);
     delete plan;
 }
 
@@ -1824,11 +1849,10 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         launch_dep(kr_stage, c.grid_cells, s, c, X, runoff, dt, a);
         if (c.bif) launch_dep(kr_stage_path, c.grid_paths, s, c, X, a);
         launch_dep(kr_limit, c.grid_cells, s, c, X, dt, a);
-        // cells, then (with paths) the path direction threads in trailing blocks
+        // cells, then the path and dam direction threads in trailing blocks
         const int path_blocks = c.bif ? (int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock) : 0;
-        launch_dep(kr_momentum, c.grid_cells + path_blocks, s, c, X, runoff, dt, a);
-        if (c.res && c.ND > 0)
-            launch_dep(kr_dam, (int)((c.ND * kDamDirs + kBlock - 1) / kBlock), s, c, X, runoff, dt, a);
+        const int dam_blocks = (c.res && c.ND > 0) ? (int)((c.ND * kDamDirs + kBlock - 1) / kBlock) : 0;
+        launch_dep(kr_momentum, c.grid_cells + path_blocks + dam_blocks, s, c, X, runoff, dt, a);
     }
     return launch_status();
 }
