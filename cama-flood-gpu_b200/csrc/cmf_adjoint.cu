@@ -207,7 +207,7 @@ struct Ctx {
     const int* dam_slot;
     // slot geometry (doubles); lev_off: the pre-levee stage of the levee
     // cells [4][NLV] (river/flood storage, river/flood depth) that ka_levee
-    // records in the slot of its sub-step for kr_levee_prep
+    // records in the slot of its sub-step for kr_levee
     long slot_len, path_off, lev_off;
     int grid_cells, grid_paths;
 };
@@ -1012,27 +1012,30 @@ __device__ __forceinline__ double* lam_path(const Ctx& c, double* lam, int f)
 }
 __device__ __forceinline__ double* pscr(const Ctx& c, double* scr) { return scr + (long)kCellScratch * c.N; }
 // path scratch: LRCB [P], LRDB [P], BLIMB [P*L], BCSDB [P*L], PEB [8P];
-// levee scratch: LEVB [6*NLV], LEVIN [10*NLV]
+// levee scratch: LEVB [6*NLV]
 __device__ __forceinline__ double* lrcb(const Ctx& c, double* scr) { return pscr(c, scr); }
 __device__ __forceinline__ double* lrdb(const Ctx& c, double* scr) { return pscr(c, scr) + c.P; }
 __device__ __forceinline__ double* blimb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P; }
 __device__ __forceinline__ double* bcsdb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P + c.P * c.L; }
 __device__ __forceinline__ double* peb(const Ctx& c, double* scr) { return pscr(c, scr) + 2 * c.P + 2 * c.P * c.L; }
 __device__ __forceinline__ double* levb(const Ctx& c, double* scr) { return peb(c, scr) + 8 * c.P; }
-__device__ __forceinline__ double* levin(const Ctx& c, double* scr) { return levb(c, scr) + 6 * c.NLV; }
 // dam scratch: the deferred dam adjoints, DAMB [ND][kDamDirs]
-__device__ __forceinline__ double* damb(const Ctx& c, double* scr) { return levin(c, scr) + 10 * c.NLV; }
+__device__ __forceinline__ double* damb(const Ctx& c, double* scr) { return levb(c, scr) + 6 * c.NLV; }
 
 // Apply the adjoints the later sub-step's momentum (downstream depth) and path
 // kernels (end states) left for cell i; returns nothing, updates lam / grad.
-__device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a)
+// The pending depth / end-state adjoints of cell i gathered from what the
+// later sub-step's momentum and path reverses left in the scratch.
+__device__ __forceinline__ void pending_sums(const Ctx& c, long i, const Adj& a, double& rdep_bar,
+                                             double& pdep_bar, double& tot_bar)
 {
     const long N = c.N;
-    double* lam = a.lam;
     double wsum = 0.0;
     const int c0 = c.up[i], c1 = up_end(c, i);
     for (int u = c0; u < c1; ++u) wsum += a.scr[S_WDNB * N + u];
-    double rdep_bar = wsum, pdep_bar = 0.0, tot_bar = 0.0;
+    rdep_bar = wsum;
+    pdep_bar = 0.0;
+    tot_bar = 0.0;
     const uint8_t fl = c.flags[i];
     if (c.bif && (fl & CMF_CELL_BIFURCATION)) {
         const double* pe = peb(c, a.scr);
@@ -1044,6 +1047,15 @@ __device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a
             tot_bar += q[3];
         }
     }
+}
+
+__device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a)
+{
+    const long N = c.N;
+    double* lam = a.lam;
+    const uint8_t fl = c.flags[i];
+    double rdep_bar, pdep_bar, tot_bar;
+    pending_sums(c, i, a, rdep_bar, pdep_bar, tot_bar);
     lam[F_RDEP * N + i] += rdep_bar;
     a.grad[G_RH * N + i] -= rdep_bar;
     if (c.ND > 0 && (fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) {
@@ -1071,38 +1083,52 @@ __device__ __forceinline__ void apply_pending(const Ctx& c, long i, const Adj& a
     }
 }
 
-// Levee re-partition reversed, over the levee list, before kr_stage.
-// kr_levee_prep completes lambda_{k+1} of the levee cell and recomputes its
-// flood stage; kr_levee runs one dual pass per levee and input direction and
-// leaves the adjoints of the flood-stage outputs (and of river width/height)
-// for kr_stage.  Compact kernels keep the long dual passes out of the
-// per-cell stage kernel.
-__global__ void __launch_bounds__(kBlock) kr_levee_prep(const Ctx c, const double* X,
-                                                        const double* runoff, double dt, Adj a)
+// lambda_{k+1} of cell i's river/flood/protected storage and river/flood/
+// protected depth with its pending terms added, in apply_pending's order,
+// without writing them (kr_stage applies them).
+__device__ __forceinline__ void pending_view(const Ctx& c, long i, const Adj& a, double (&q)[6])
 {
-    pdl_begin();
-    const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= c.NLV) return;
     const long N = c.N;
-    const long i = c.lci[l];
-    apply_pending(c, i, a);
     const double* lam = a.lam;
-    // the flood-stage result the levee re-partitioned, recorded by ka_levee
-    const double* rec = X + c.lev_off;
-    double* q = levin(c, a.scr) + 10 * l;
-    q[0] = rec[l];
-    q[1] = rec[c.NLV + l];
-    q[2] = rec[2 * c.NLV + l];
-    q[3] = rec[3 * c.NLV + l];
-    q[4] = lam[F_RS * N + i];
-    q[5] = lam[F_FS * N + i];
-    q[6] = lam[F_PS * N + i];
-    q[7] = lam[F_RDEP * N + i];
-    q[8] = lam[F_FDEP * N + i];
-    q[9] = lam[F_PDEP * N + i];
+    const uint8_t fl = c.flags[i];
+    double rdep_bar, pdep_bar, tot_bar;
+    pending_sums(c, i, a, rdep_bar, pdep_bar, tot_bar);
+    double rs = lam[F_RS * N + i], fs = lam[F_FS * N + i], ps = lam[F_PS * N + i];
+    double rdep = lam[F_RDEP * N + i], fdep = lam[F_FDEP * N + i], pdep = lam[F_PDEP * N + i];
+    rdep += rdep_bar;
+    if (c.ND > 0 && (fl & (CMF_CELL_RESERVOIR | CMF_CELL_DAM_UPSTREAM))) {
+        const double* db = damb(c, a.scr) + (long)kDamDirs * c.dam_slot[i];
+        if (fl & CMF_CELL_RESERVOIR) {
+            rs += db[0];
+            fs += db[1];
+        } else {
+            rdep += db[0];
+            fdep += db[1];
+            rs += db[2];
+            fs += db[3];
+        }
+    }
+    if (pdep_bar != 0.0) pdep += pdep_bar;
+    if (tot_bar != 0.0) {
+        rs += tot_bar;
+        fs += tot_bar;
+        if (!(c.res && (fl & CMF_CELL_RESERVOIR))) ps += tot_bar;
+    }
+    q[0] = rs;
+    q[1] = fs;
+    q[2] = ps;
+    q[3] = rdep;
+    q[4] = fdep;
+    q[5] = pdep;
 }
 
-__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx c, Adj a)
+// Levee re-partition reversed, over the levee list, before kr_stage: one dual
+// pass per levee and input direction, on the flood-stage result from the tape
+// and lambda_{k+1} of the outputs (with the pending terms, which kr_stage then
+// applies), leaving the adjoints of the flood-stage outputs (and of river
+// width/height) for kr_stage.  A compact kernel keeps the long dual passes
+// out of the per-cell stage kernel.
+__global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx c, const double* X, Adj a)
 {
     pdl_begin();
     // threads [0, 4 NLV): the four state directions of each levee; then
@@ -1122,9 +1148,13 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx
         j = 4 + (int)(u & 1);
     }
     const long i = c.lci[l];
-    const double* q = levin(c, a.scr) + 10 * l;
+    // the flood-stage result the levee re-partitioned (recorded by ka_levee)
+    // and lambda_{k+1} of the outputs with their pending terms
+    const double* rec = X + c.lev_off;
+    double lb[6];
+    pending_view(c, i, a, lb);
     Dual x[4], y[6];
-    for (int k = 0; k < 4; ++k) x[k] = {q[k], k == j ? 1.0 : 0.0};
+    for (int k = 0; k < 4; ++k) x[k] = {rec[k * nlv + l], k == j ? 1.0 : 0.0};
     double ffr = 0.0;
     if (j < 4) {
         levee_part<Dual, double>(c, i, x, c.rw[i], c.rh[i], ffr, y);
@@ -1133,7 +1163,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_levee(const Ctx
         levee_part<Dual, Dual>(c, i, x, rw, rh, ffr, y);
     }
     double v = 0.0;
-    for (int o = 0; o < 6; ++o) v += q[4 + o] * y[o].d;
+    for (int o = 0; o < 6; ++o) v += lb[o] * y[o].d;
     levb(c, a.scr)[6 * l + j] = v;
 }
 
@@ -1152,7 +1182,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_stage(const Ctx
     const bool lev_cell = c.lev && (fl & CMF_CELL_LEVEE);
     const bool res_cell = c.res && (fl & CMF_CELL_RESERVOIR);
 
-    if (!lev_cell) apply_pending(c, i, a);   // levee cells: done by kr_levee
+    apply_pending(c, i, a);
     double L_rs = lam[F_RS * N + i], L_fs = lam[F_FS * N + i];
     const double L_rout = lam[F_ROUT * N + i], L_fout = lam[F_FOUT * N + i];
     double L_rdep = lam[F_RDEP * N + i], L_fdep = lam[F_FDEP * N + i];
@@ -1645,7 +1675,7 @@ int launch_status()
 
 long scratch_len(const Ctx& c)
 {
-    return (long)kCellScratch * c.N + 2 * c.P + 2 * c.P * c.L + 8 * c.P + 16 * c.NLV + kDamDirs * c.ND;
+    return (long)kCellScratch * c.N + 2 * c.P + 2 * c.P * c.L + 8 * c.P + 6 * c.NLV + kDamDirs * c.ND;
 }
 
 }  // namespace
@@ -1843,8 +1873,7 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
     for (int k = num_sub_steps - 1; k >= 0; --k) {
         const double* X = tape + (long)k * stride;
         if (c.lev && c.NLV > 0) {
-            launch_dep(kr_levee_prep, (int)((c.NLV + kBlock - 1) / kBlock), s, c, X, runoff, dt, a);
-            launch_dep(kr_levee, (int)((c.NLV * 6 + kBlock - 1) / kBlock), s, c, a);
+            launch_dep(kr_levee, (int)((c.NLV * 6 + kBlock - 1) / kBlock), s, c, X, a);
         }
         launch_dep(kr_stage, c.grid_cells, s, c, X, runoff, dt, a);
         if (c.bif) launch_dep(kr_stage_path, c.grid_paths, s, c, X, a);
