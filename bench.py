@@ -347,7 +347,8 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
     intervals, discharge at 500 cells with upstream area > 1000 km^2,
     relative-misfit loss against a run with river Manning x lognormal(0.2).
     Both are timed with CUDA events on the same GPU from the same spun-up
-    state; the gradient run includes its checkpointed forward."""
+    state, three interleaved repetitions, medians; the gradient run includes
+    its checkpointed forward."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn, topology
     from cmfb200.adjoint import AdjointRouting
@@ -387,16 +388,23 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
     fwd()
     fwd_adj()                                 # warm-up (allocations, lazy init)
     torch.cuda.synchronize(device)
-    ev[0].record(stream)
-    fwd()
-    ev[1].record(stream)
-    torch.cuda.synchronize(device)
-    ev[2].record(stream)
-    fwd_adj()
-    ev[3].record(stream)
-    torch.cuda.synchronize(device)
-    t_fwd = ev[0].elapsed_time(ev[1]) / 1e3
-    t_adj = ev[2].elapsed_time(ev[3]) / 1e3
+    # three interleaved repetitions, medians reported (single runs vary by a
+    # few per cent with the GPU's power state)
+    reps = 3
+    tf, ta = [], []
+    for _ in range(reps):
+        ev[0].record(stream)
+        fwd()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        ev[2].record(stream)
+        fwd_adj()
+        ev[3].record(stream)
+        torch.cuda.synchronize(device)
+        tf.append(ev[0].elapsed_time(ev[1]) / 1e3)
+        ta.append(ev[2].elapsed_time(ev[3]) / 1e3)
+    t_fwd = statistics.median(tf)
+    t_adj = statistics.median(ta)
     # the product's own fp64 forward (interval graphs) over the same window
     snap = {k: v.clone() for k, v in model.state_tensors().items()}
     b = model.base
@@ -412,11 +420,14 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
 
     product_fwd()
     torch.cuda.synchronize(device)
-    ev[0].record(stream)
-    product_fwd()
-    ev[1].record(stream)
-    torch.cuda.synchronize(device)
-    t_prod = ev[0].elapsed_time(ev[1]) / 1e3
+    tp = []
+    for _ in range(reps):
+        ev[0].record(stream)
+        product_fwd()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        tp.append(ev[0].elapsed_time(ev[1]) / 1e3)
+    t_prod = statistics.median(tp)
     # sub-step count of the window (the CFL counts of the primal run)
     _, _, counts, _, _ = eng._forward(params["river_manning"], params["flood_manning"],
                                       params["river_height"], params["river_width"], forcing,
@@ -426,6 +437,7 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
     n = eng.N
     return {"fwd_value": n * subs / t_fwd, "fwd_adj_value": n * subs / t_adj, "unit": UNIT,
             "fwd_adj_over_fwd": t_adj / t_fwd,
+            "repeats": reps, "fwd_adj_over_fwd_each": [a / f for a, f in zip(ta, tf)],
             "product_fwd_value": n * subs / t_prod, "fwd_adj_over_product_fwd": t_adj / t_prod,
             "catchments": n, "sub_steps": subs,
             "days": days, "checkpoint_every": checkpoint_every, "gauges": int(gauges.size),
