@@ -1,6 +1,6 @@
 // Device kernels of the B200 routing core.
 //
-// One sub-step of CaMa-Flood routing is two fused, HBM-bound kernels:
+// One sub-step of CaMa-Flood routing is four HBM-bound kernels:
 //
 //   k_momentum  per catchment (x member): local-inertial river + floodplain
 //               momentum, negative-flow limiter, dam-upstream kinematic flow
@@ -8,12 +8,19 @@
 //               multi-level path flux and its path limiter.  Writes the
 //               unlimited fluxes ("qu") to scratch and the cross-section state
 //               in place.
-//   k_stage     per catchment (x member): storage-based outflow limiter,
-//               upstream inflow as a deterministic gather over the catchment's
-//               contiguous upstream range, bifurcation net flux, fp64 storage
-//               update, flood-stage diagnosis over the floodplain table, levee
-//               re-partition and the fp64 water budget; per path: the
-//               limit-rate scaling of the level fluxes.
+//   k_limit     per catchment (x member): the storage-based outflow limit
+//               rate from the unlimited fluxes of the cell, its upstream range
+//               and its bifurcation ends.
+//   k_stage     per catchment (x member): limited fluxes, upstream inflow as a
+//               deterministic gather over the catchment's contiguous upstream
+//               range, bifurcation net flux, fp64 storage update, flood-stage
+//               diagnosis over the floodplain table and the fp64 water budget;
+//               per path: the limit-rate scaling of the level fluxes.
+//   k_levee     per levee (x member): the levee re-partition of the levee
+//               cells' flood-stage result.
+//
+// After them, with output statistics attached, k_stats_accumulate folds the
+// sub-step into the statistics.
 //
 // Catchments are stored breadth-first from the mouths, so the upstream cells
 // of p are [up[p], up[p+1]) and no upstream index array exists.  Every float

@@ -6,7 +6,9 @@
 // device->host `.item()` of the sub-step count (:122):
 //
 //   begin -> [cfl] -> plan (n, dt per member, while-condition)
-//         -> WHILE(cond) { momentum -> stage (last block: k += 1, cond = k < n) }
+//         -> WHILE(cond) { momentum -> limit -> stage -> [levee]
+//                          (last block of the last of them: k += 1, cond = k < n)
+//                          -> [statistics] }
 //         -> end (storage copy-back for odd counts, current_step)
 //         -> [budget flush]
 //
