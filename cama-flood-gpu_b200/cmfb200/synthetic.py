@@ -280,9 +280,10 @@ def runoff_mapping(network: Network, grid_shape=(720, 1440), seed: int = 0, max_
                    extra_rows: int = 0) -> dict:
     """A runoff mapping table in the reference's `.npz` layout
     (cmfgpu/params/export_bin.py:955-983) for `network` on a ny x nx runoff
-    grid: every catchment draws 1..max_cells cells of the 2x2 block at its grid
-    position (catchments sweep the grid in generator order, so neighbours in
-    the river tree share nearby cells), weights split its area.  Rows are
+    grid: every catchment draws 1..max_cells cells of the 2x2 block (3x3 when
+    max_cells > 4, up to 9) at its grid position (catchments sweep the grid in
+    generator order, so neighbours in the river tree share nearby cells),
+    weights split its area.  Rows are
     shuffled against the network order and `extra_rows` rows for catchments
     outside the network are added, as a global table seen by one domain."""
     rng = np.random.default_rng([seed, 271828])
@@ -296,11 +297,14 @@ def runoff_mapping(network: Network, grid_shape=(720, 1440), seed: int = 0, max_
     base = (np.arange(n, dtype=np.int64) * G) // max(n, 1)
     bx, by = base % nx, base // nx
     cnt = rng.integers(1, max_cells + 1, size=n)
-    offs = np.array([[0, 0], [1, 0], [0, 1], [1, 1]], dtype=np.int64)
-    perm = np.argsort(rng.random((n, 4)), axis=1)          # which block cells, in which order
+    side = 2 if max_cells <= 4 else 3                      # 2x2 block, or 3x3 for up to 9 cells
+    if max_cells > side * side:
+        raise ValueError("max_cells is at most 9")
+    offs = np.array([[dx, dy] for dy in range(side) for dx in range(side)], dtype=np.int64)
+    perm = np.argsort(rng.random((n, side * side)), axis=1)  # which block cells, in which order
     rows = np.repeat(np.arange(n), cnt)
     slot = np.arange(rows.size) - np.repeat(np.cumsum(cnt) - cnt, cnt)
-    o = offs[perm[rows, slot % 4]]
+    o = offs[perm[rows, slot % (side * side)]]
     cx = np.minimum(bx[rows] + o[:, 0], nx - 1)
     cy = np.minimum(by[rows] + o[:, 1], ny - 1)
     frac = rng.gamma(2.0, 1.0, size=rows.size)

@@ -169,3 +169,20 @@ def test_full_size_linearity_and_volume(device):
     rp, col, w, _ = local_csr(tab, net.fields["catchment_id"][:2000])
     ref = OF.map_grid(rp, col, w, x.reshape(2, -1).cpu().numpy())
     np.testing.assert_array_equal(y[:, :2000].cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("grid_dtype", [np.float32, np.float64])
+def test_rows_with_many_entries(grid_dtype, device):
+    """Rows of up to 9 entries (a 3x3 block of runoff cells), bit-exact with
+    the oracle."""
+    net = syn.generate(syn.NetworkSpec(10_000, seed=23))
+    tab = syn.runoff_mapping(net, (50, 80), seed=23, max_cells=9)
+    cid = net.fields["catchment_id"]
+    m = build_local_mapping(tab, cid, device)
+    rp, col, w, _ = local_csr(tab, cid)
+    assert np.diff(rp).max() > 4
+    grid = syn.gridded_runoff((50, 80), 6, seed=2).astype(grid_dtype)
+    got = apply_mapping(m, torch.as_tensor(grid, device=device), dtype=torch.float64,
+                        unit_factor=86400000.0)
+    ref = OF.map_grid(rp, col, w, grid.reshape(6, -1), unit_factor=86400000.0)
+    np.testing.assert_array_equal(got.cpu().numpy(), ref)
