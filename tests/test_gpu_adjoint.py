@@ -163,3 +163,52 @@ def test_gradients_match_finite_differences(case, device):
             ad = flat[c].item()
             ok = any(abs(ad - fd(name, c, h)) <= 1e-3 * abs(ad) for h in (1e-4, 1e-6))
             assert ok, (name, c, ad, fd(name, c, 1e-4), fd(name, c, 1e-6))
+
+
+def test_gradients_match_finite_differences_random_cells(device):
+    """The benchmark definition's check at reduced size: central differences
+    at 50 random cells per parameter (river and floodplain Manning, river
+    height, river width, runoff of the first day), full physics, fp64.  A cell
+    matches when |ad - fd| <= 1e-3 * max(|ad|, 1e-3 * max|grad of that field|)
+    at h = 1e-4 relative, or at h = 1e-6 where the larger step crosses a branch
+    of the piecewise physics."""
+    net, model, eng, forcing = _setup(device, "full", n=4000, seed=29)
+    params = eng.parameters()
+    state0 = eng.initial_state()
+    q_obs = _observed(eng, params, forcing, state0)
+    p = {k: v.clone().requires_grad_(True) for k, v in params.items()}
+    forc = forcing.clone().requires_grad_(True)
+    q, _ = eng.window(p, forc, state0)
+    grads = torch.autograd.grad(_loss(q, q_obs), [p[k] for k in PARAMS] + [forc])
+
+    def loss_at(pp, ff):
+        qq, _ = eng.forward_only(pp, ff, state0)
+        return float(_loss(qq, q_obs))
+
+    def fd(name, c, h_rel):
+        base = forcing[0, c].item() if name == "runoff" else params[name][c].item()
+        h = h_rel * abs(base)
+        if h == 0.0:
+            return 0.0
+        vals = []
+        for sign in (1, -1):
+            pp = {k: v.clone() for k, v in params.items()}
+            ff = forcing.clone()
+            if name == "runoff":
+                ff[0, c] += sign * h
+            else:
+                pp[name][c] += sign * h
+            vals.append(loss_at(pp, ff))
+        return (vals[0] - vals[1]) / (2 * h)
+
+    rng = np.random.default_rng(29)
+    failures = []
+    for name, g in zip(list(PARAMS) + ["runoff"], grads):
+        flat = (g[0] if name == "runoff" else g).detach()
+        gmax = float(flat.abs().max())
+        for c in rng.choice(eng.N, size=50, replace=False).tolist():
+            ad = flat[c].item()
+            tol = 1e-3 * max(abs(ad), 1e-3 * gmax)
+            if not any(abs(ad - fd(name, c, h)) <= tol for h in (1e-4, 1e-6)):
+                failures.append((name, c, ad, fd(name, c, 1e-4), fd(name, c, 1e-6)))
+    assert not failures, failures[:5]
