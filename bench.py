@@ -448,6 +448,76 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
                         "in fp64 (interval graphs) over the same window"}
 
 
+def adjoint_fd_check(device, days: int, cells: int, seed: int = 5) -> dict:
+    """Central finite differences of the calibration loss on the 250k
+    full-physics network at `cells` random cells per parameter (river and
+    floodplain Manning, river height, river width, runoff of the first day)
+    against the CUDA adjoint: h = 1e-4 relative, retried at 1e-6 where the
+    step crosses a branch of the piecewise physics; a cell passes when
+    |ad - fd| <= 1e-3 * max(|ad|, 1e-3 * max|grad of that field|)."""
+    import torch
+    from cmfb200 import CaMaFlood, synthetic as syn
+    from cmfb200.adjoint import AdjointRouting, PARAMS
+    net = syn.generate(syn.CONFIGS["full_250k"]["spec"])
+    model = CaMaFlood(device=device, input_proxy=net.fields,
+                      opened_modules=net.opened_modules, precision="float64")
+    model.set_inputs(torch.as_tensor(syn.daily_runoff(net, 0)[model.order]).to(device))
+    model.step_advance()
+    rng = np.random.default_rng(seed)
+    gauges = np.sort(rng.choice(model.num_catchments, size=500, replace=False))
+    eng = AdjointRouting(model, gauges)
+    forcing = torch.as_tensor(np.stack([syn.daily_runoff(net, 1 + d)[model.order]
+                                        for d in range(days)]), dtype=torch.float64, device=device)
+    params = eng.parameters()
+    state0 = eng.initial_state()
+    truth = dict(params)
+    truth["river_manning"] = params["river_manning"] * torch.as_tensor(
+        np.exp(0.2 * rng.standard_normal(eng.N)), device=device)
+    q_obs, _ = eng.forward_only(truth, forcing, state0)
+
+    def loss(q):
+        return (((q - q_obs) / q_obs) ** 2).sum()
+
+    p = {k: v.clone().requires_grad_(True) for k, v in params.items()}
+    f = forcing.clone().requires_grad_(True)
+    q, _ = eng.window(p, f, state0)
+    grads = torch.autograd.grad(loss(q), [p[k] for k in PARAMS] + [f])
+
+    def fd(name, c, h_rel):
+        base = forcing[0, c].item() if name == "runoff" else params[name][c].item()
+        h = h_rel * abs(base)
+        if h == 0.0:
+            return 0.0
+        vals = []
+        for sign in (1, -1):
+            pp = {k: v.clone() for k, v in params.items()}
+            ff = forcing.clone()
+            if name == "runoff":
+                ff[0, c] += sign * h
+            else:
+                pp[name][c] += sign * h
+            vals.append(float(loss(eng.forward_only(pp, ff, state0)[0])))
+        return (vals[0] - vals[1]) / (2 * h)
+
+    passed, total, worst, at_small_h = 0, 0, 0.0, 0
+    for name, g in zip(list(PARAMS) + ["runoff"], grads):
+        flat = (g[0] if name == "runoff" else g).detach()
+        gmax = float(flat.abs().max())
+        for c in rng.choice(eng.N, size=cells, replace=False).tolist():
+            ad = flat[c].item()
+            scale = max(abs(ad), 1e-3 * gmax)
+            e1 = abs(ad - fd(name, c, 1e-4)) / scale
+            err = e1 if e1 <= 1e-3 else min(e1, abs(ad - fd(name, c, 1e-6)) / scale)
+            at_small_h += int(e1 > 1e-3 and err <= 1e-3)
+            passed += int(err <= 1e-3)
+            total += 1
+            worst = max(worst, err)
+    model.close()
+    return {"cells_per_field": cells, "fields": list(PARAMS) + ["runoff"], "passed": passed,
+            "total": total, "passed_at_h_1e-6": at_small_h, "max_scaled_error": worst,
+            "days": days, "catchments": eng.N}
+
+
 def run_reference(args) -> None:
     """CPU restatement of the reference path on all host cores (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -680,6 +750,8 @@ def run_ours(args) -> None:
     if world == 1 and args.adjoint_days > 0:
         model.close()
         adjoint = adjoint_compare(device, args.adjoint_days)
+        if args.adjoint_fd_cells > 0:
+            adjoint["fd_check"] = adjoint_fd_check(device, args.adjoint_fd_days, args.adjoint_fd_cells)
 
     if world > 1:
         dist.barrier()
@@ -734,6 +806,11 @@ def main() -> None:
                     help="members of the batched-vs-looped comparison (0 skips it)")
     ap.add_argument("--adjoint-days", type=int, default=30,
                     help="daily intervals of the forward+adjoint comparison (0 = skip)")
+    ap.add_argument("--adjoint-fd-cells", type=int, default=0,
+                    help="random cells per parameter of a finite-difference check of the "
+                         "adjoint on the 250k network (0 = skip)")
+    ap.add_argument("--adjoint-fd-days", type=int, default=3,
+                    help="window length of that check")
     ap.add_argument("--forcing-steps", type=int, default=24,
                     help="steps per chunk of the gridded-runoff forcing map leg (0 = skip)")
     ap.add_argument("--no-statistics", dest="statistics", action="store_false",
