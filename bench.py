@@ -265,14 +265,17 @@ def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: flo
             "sub_steps": sub, "finite": ok}
 
 
-def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -> dict:
+def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
+                     member_tile: int = 2, block: int = 128) -> dict:
     """The batched-ensemble workload: `members` members of a `basins`-basin
     network (~`catchments` catchments per member, 6M by default; runoff and
     river Manning perturbed per member, daily forcing, per-member dt).  One
     simulated day of the 30-day window (a bounded sample) in a single
     member-innermost model (one launch per phase) against the same members run
     one after another as plain models, both from the same initial state on the
-    same GPU."""
+    same GPU.  The batched model runs `member_tile` members of a catchment per
+    thread in CTAs of `block` threads (member_tile 0: the autotuner picks both
+    on the first day); the looped plain models keep their default CTA size."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn
     net = syn.generate_basins(basins, catchments, seed=3)
@@ -281,7 +284,8 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
     manning = (net.fields["river_manning"][:, None] * mfac).astype(np.float32)
     mods = ["base", "adaptive_time"]
     ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=mods,
-                    num_members=members, batched_fields={"river_manning": manning})
+                    num_members=members, batched_fields={"river_manning": manning},
+                    **({"BLOCK_SIZE": block} if member_tile > 0 else {}))
     order = ens.order
     rm = (syn.daily_runoff(net, 0)[:, None] * rfac).astype(np.float32)[order]
     forcing = torch.as_tensor(rm).to(device)
@@ -293,6 +297,10 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
             v.copy_(state[k])
 
     ens.set_inputs(forcing)
+    if member_tile > 0:
+        ens.set_member_tile(member_tile)
+    else:
+        ens.autotune_block_size(sub_steps=2)
     ens.step_advance()                      # builds the interval graph
     reset(ens, init)
     torch.cuda.synchronize(device)
@@ -304,6 +312,7 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
     torch.cuda.synchronize(device)
     t_batched = a.elapsed_time(b) / 1e3
     n_batched = int(ens.sub_step_counts().sum().item())
+    tile, block = ens.member_tile, ens.block_size
     ens.close()
     del ens, init
 
@@ -333,6 +342,7 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500) -
     looped = n * n_looped / t_looped
     return {"value": batched, "looped_value": looped, "speedup": batched / looped,
             "unit": UNIT, "members": members, "catchments_per_member": n, "basins": basins,
+            "member_tile": tile, "block": block,
             "sub_steps_per_member_mean": n_batched / members,
             "workload": "1 day (a sample of the 30-day window) of a member-innermost ensemble "
                         "(runoff x lognormal(0.3), river Manning x U(0.8,1.2) per member) vs "
@@ -744,7 +754,9 @@ def run_ours(args) -> None:
     ensemble = None
     if world == 1 and args.ensemble_members > 0:
         model.close()
-        ensemble = ensemble_compare(device, args.ensemble_members, args.ensemble_catchments)
+        ensemble = ensemble_compare(device, args.ensemble_members, args.ensemble_catchments,
+                                    member_tile=args.ensemble_member_tile,
+                                    block=args.ensemble_block)
 
     adjoint = None
     if world == 1 and args.adjoint_days > 0:
@@ -818,6 +830,12 @@ def main() -> None:
     ap.add_argument("--ensemble-catchments", type=int, default=6_000_000,
                     help="catchments per member of that comparison (the benchmark's ensemble "
                          "workload: ~6M in 500 basins)")
+    ap.add_argument("--ensemble-member-tile", type=int, default=2,
+                    help="members of a catchment per thread in the batched model "
+                         "(0: autotuned block size and tile); 2 with 128-thread CTAs is "
+                         "the fastest pair measured at 64 members x 6M catchments")
+    ap.add_argument("--ensemble-block", type=int, default=128,
+                    help="threads per CTA of the batched model")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -167,6 +167,8 @@ def lib() -> ctypes.CDLL:
     h.cmf_plan_create.argtypes = [ctypes.POINTER(CmfView), ctypes.POINTER(_P)]
     h.cmf_plan_destroy.restype = None
     h.cmf_plan_destroy.argtypes = [_P]
+    h.cmf_plan_set_member_tile.restype = ctypes.c_int
+    h.cmf_plan_set_member_tile.argtypes = [_P, _I32]
     h.cmf_step_interval.restype = ctypes.c_int
     h.cmf_step_interval.argtypes = [_P, _P, _F64, _I32]
     h.cmf_phase_momentum.restype = ctypes.c_int

@@ -169,6 +169,7 @@ class CaMaFlood:
         self.max_sub_step_seconds = float(max_sub_step_seconds)
         self.max_sub_steps_cap = int(max_sub_steps_cap)
         self.budget_enabled = bool(budget) or "log" in mods
+        self.member_tile = 1
         self._plan = None
         self._prepare(dict(input_proxy), dict(batched_fields or {}))
         self._upload()
@@ -548,6 +549,8 @@ class CaMaFlood:
         plan = ctypes.c_void_p()
         _lib.check(lib.cmf_plan_create(ctypes.byref(view), ctypes.byref(plan)), "plan_create")
         self._plan = plan
+        if self.member_tile != 1:
+            _lib.check(lib.cmf_plan_set_member_tile(plan, self.member_tile), "plan_set_member_tile")
         self._attach_statistics()
 
     # ------------------------------------------------------------------ #
@@ -675,13 +678,23 @@ class CaMaFlood:
         self.block_size = int(block_size)
         self._create_plan()
 
+    def set_member_tile(self, width: int) -> None:
+        """Members per thread of the member-batched kernels (a divisor of
+        num_members; 1 for one member).  Results do not depend on it."""
+        width = int(width)
+        if width < 1 or self.num_members % width or (self.num_members == 1 and width != 1):
+            raise ValueError(f"member tile {width} must divide num_members={self.num_members}")
+        _lib.check(_lib.lib().cmf_plan_set_member_tile(self._plan, width), "plan_set_member_tile")
+        self.member_tile = width
+
     def autotune_block_size(self, candidates=None, sub_steps: int = 6,
-                            cache_path: Optional[str] = None) -> dict:
-        """Measure the candidate CTA sizes on this network and keep the
-        fastest (cmfb200.autotune.tune_block_size); the state is unchanged."""
+                            cache_path: Optional[str] = None, tile_candidates=None) -> dict:
+        """Measure the candidate CTA sizes (and, with several members, member
+        tiles) on this network and keep the fastest
+        (cmfb200.autotune.tune_block_size); the state is unchanged."""
         from .autotune import DEFAULT_CANDIDATES, tune_block_size
         return tune_block_size(self, candidates or DEFAULT_CANDIDATES, sub_steps,
-                               cache_path=cache_path)
+                               cache_path=cache_path, tile_candidates=tile_candidates)
 
     def flush_budget(self) -> None:
         _lib.check(_lib.lib().cmf_budget_flush(self._plan, self._stream()), "budget_flush")

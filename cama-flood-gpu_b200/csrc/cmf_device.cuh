@@ -66,6 +66,7 @@ struct Dev {
     long N;
     int M;
     int mshift;   // log2(M) when M is a power of two, else -1
+    int mtile;    // member-tile width: consecutive members of a cell per thread (divides M)
     int K;
     long P;
     int L;
@@ -128,6 +129,12 @@ struct Dev {
 // ---------------------------------------------------------------------------
 template <bool ONE>
 __device__ __forceinline__ long ix(long i, int m, int M) { return ONE ? i : i * (long)M + m; }
+
+// Member-tile width of the batched kernels (1 for one member): thread t0
+// handles elements t0 * W .. t0 * W + W - 1 of the member-innermost order,
+// W consecutive members of one cell, whose cell-shared loads then hit L1.
+template <typename REAL, bool ONE>
+__device__ __forceinline__ int mtile_of(const Dev<REAL>& v) { return ONE ? 1 : v.mtile; }
 
 // (item, member) of flat thread index t over [items, M]: a shift and a mask
 // when M is a power of two, a division otherwise.
@@ -507,19 +514,26 @@ __device__ __forceinline__ void momentum_path(const Dev<REAL>& v, long p, int m,
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF>
 __global__ void __launch_bounds__(256, CMF_MOMENTUM_MIN_BLOCKS(REAL, ONE)) k_momentum(const Dev<REAL> v, int kh, int force_diag)
 {
+    const int W = mtile_of<REAL, ONE>(v);
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
-        long t = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
-        if (t >= v.P * (long)v.M) return;
-        int m;
-        long p = split_member<ONE>(v, t, m);
-        momentum_path<REAL, ONE, RES, LEV>(v, p, m, kh);
+        const long t0 = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
+        for (int w = 0; w < W; ++w) {
+            const long t = t0 * W + w;
+            if (t >= v.P * (long)v.M) return;
+            int m;
+            long p = split_member<ONE>(v, t, m);
+            momentum_path<REAL, ONE, RES, LEV>(v, p, m, kh);
+        }
         return;
     }
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= v.N * (long)v.M) return;
-    int m;
-    long i = split_member<ONE>(v, t, m);
-    momentum_cell<REAL, ONE, RES, LEV, BIF>(v, i, m, kh, force_diag);
+    const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int w = 0; w < W; ++w) {
+        const long t = t0 * W + w;
+        if (t >= v.N * (long)v.M) return;
+        int m;
+        long i = split_member<ONE>(v, t, m);
+        momentum_cell<REAL, ONE, RES, LEV, BIF>(v, i, m, kh, force_diag);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1060,16 +1074,20 @@ __device__ __forceinline__ void stage_path(const Dev<REAL>& v, long p, int m, in
 template <typename REAL, bool ONE, bool BIF>
 __global__ void __launch_bounds__(256, (sizeof(REAL) == 4 ? 8 : 4)) k_limit(const Dev<REAL> v, int kh)
 {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= v.N * (long)v.M) return;
-    int m;
-    long i = split_member<ONE>(v, t, m);
-    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
-    if (!st.active) return;
-    const int k = st.k;
-    const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
-    const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
-    v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
+    const int W = mtile_of<REAL, ONE>(v);
+    const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int w = 0; w < W; ++w) {
+        const long t = t0 * W + w;
+        if (t >= v.N * (long)v.M) return;
+        int m;
+        long i = split_member<ONE>(v, t, m);
+        const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
+        if (!st.active) continue;
+        const int k = st.k;
+        const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
+        const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
+        v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
+    }
 }
 
 // Interval loop control, run by the last kernel of a sub-step: the last
@@ -1101,8 +1119,11 @@ template <typename REAL, bool ONE>
 __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int advance)
 {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < v.NLV * (long)v.M) {
+    const int W = mtile_of<REAL, ONE>(v);
+    const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int w = 0; w < W; ++w) {
+        const long t = t0 * W + w;
+        if (t >= v.NLV * (long)v.M) break;
         int m;
         const long li = split_member<ONE>(v, t, m);
         const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
@@ -1159,9 +1180,12 @@ template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
 __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int set_cond)
 {
+    const int W = mtile_of<REAL, ONE>(v);
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
-        long t = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
-        if (t < v.P * (long)v.M) {
+        const long t0 = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
+        for (int w = 0; w < W; ++w) {
+            const long t = t0 * W + w;
+            if (t >= v.P * (long)v.M) break;
             int m;
             long p = split_member<ONE>(v, t, m);
             stage_path<REAL, ONE, BIF>(v, p, m, kh);
@@ -1170,8 +1194,10 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
         double bud[kBudgetTerms];
 #pragma unroll
         for (int q = 0; q < kBudgetTerms; ++q) bud[q] = 0.0;
-        long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (t < v.N * (long)v.M) {
+        const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+        for (int w = 0; w < W; ++w) {
+            const long t = t0 * W + w;
+            if (t >= v.N * (long)v.M) break;
             int m;
             long i = split_member<ONE>(v, t, m);
             stage_cell<REAL, ONE, RES, LEV, BIF, BUDGET>(v, i, m, kh, force_diag, bud);

@@ -150,6 +150,8 @@ struct CmfPlan {
     int cell_blocks;
     int path_blocks;
     int levee_blocks;
+    int layout_blocks;  // cell_blocks the workspace layout was made with (member tile 1)
+    int mtile;          // member-tile width of the batched kernels
     // graph
     bool graph_ready;
     cudaGraph_t graph;
@@ -177,6 +179,7 @@ void fill_dev(CmfPlan* p, const Layout& L, bool packed)
     d.N = (long)v.num_catchments;
     d.M = v.num_members;
     d.mshift = -1;
+    d.mtile = p->mtile > 0 ? p->mtile : 1;
     for (int b = 0; b < 31; ++b)
         if (v.num_members == (1 << b)) d.mshift = b;
     d.K = v.num_flood_levels;
@@ -420,7 +423,7 @@ int build_graph(CmfPlan* p, double T, int fixed_n)
         if ((rc = add_kernel(&nend, g, &nwhile, 1, p->ks.end, eb, 256, args)) != CMF_OK) goto fail;
     }
     if (v.features & CMF_FEAT_BUDGET) {
-        Layout L = layout_of(&v, p->cell_blocks);
+        Layout L = layout_of(&v, p->layout_blocks);
         double* bpart = (double*)((char*)v.workspace + L.bpart);
         int* ctl = (int*)((char*)v.workspace + L.ctl);
         double* budget = v.budget;
@@ -475,7 +478,7 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
         void* args[] = {p->dev, &f, &h, &set};
         if ((rc = launch(p->ks.plan, 1, 256, args, s)) != CMF_OK) return rc;
     }
-    Layout L = layout_of(&v, p->cell_blocks);
+    Layout L = layout_of(&v, p->layout_blocks);
     int* ctl = (int*)((char*)v.workspace + L.ctl);
     int nmax = 0;
     if ((rc = check_cuda(cudaMemcpyAsync(&nmax, ctl + kCtlMaxSteps, sizeof(int),
@@ -604,7 +607,9 @@ int cmf_plan_create(const CmfView* view, CmfPlan** out)
     p->adaptive = f & CMF_FEAT_ADAPTIVE;
     p->graph_enabled = f & CMF_FEAT_GRAPH;
     p->tpb = block_of(view);
+    p->mtile = 1;
     p->cell_blocks = ceil_div((long)view->num_catchments * view->num_members, p->tpb);
+    p->layout_blocks = p->cell_blocks;
     p->path_blocks = (f & CMF_FEAT_BIFURCATION)
                          ? ceil_div((long)view->num_bifurcation_paths * view->num_members, p->tpb)
                          : 0;
@@ -613,7 +618,7 @@ int cmf_plan_create(const CmfView* view, CmfPlan** out)
                           : 0;
     const bool res = f & CMF_FEAT_RESERVOIR, lev = f & CMF_FEAT_LEVEE,
                bif = f & CMF_FEAT_BIFURCATION, bud = f & CMF_FEAT_BUDGET;
-    Layout L = layout_of(view, p->cell_blocks);
+    Layout L = layout_of(view, p->layout_blocks);
     if (p->fp64) {
         p->ks = pick_one<double>(p->one, res, lev, bif, bud);
         fill_dev<double>(p, L, true);
@@ -809,7 +814,7 @@ int cmf_budget_flush(CmfPlan* p, void* stream)
 {
     if (!p) return CMF_ERR_ARG;
     if (!(p->view.features & CMF_FEAT_BUDGET)) return CMF_OK;
-    Layout L = layout_of(&p->view, p->cell_blocks);
+    Layout L = layout_of(&p->view, p->layout_blocks);
     double* bpart = (double*)((char*)p->view.workspace + L.bpart);
     int* ctl = (int*)((char*)p->view.workspace + L.ctl);
     double* budget = p->view.budget;
@@ -817,6 +822,30 @@ int cmf_budget_flush(CmfPlan* p, void* stream)
     int cs = 0;
     void* args[] = {&bpart, &nb, &budget, &ctl, &cs};
     return launch((const void*)k_budget_flush, 1, 256, args, (cudaStream_t)stream);
+}
+
+int cmf_plan_set_member_tile(CmfPlan* p, int32_t width)
+{
+    if (!p || width < 1) return CMF_ERR_ARG;
+    const int M = p->view.num_members;
+    if (M % width != 0 || (M == 1 && width != 1)) return CMF_ERR_ARG;
+    if (width == p->mtile) return CMF_OK;
+    if (p->graph_ready) {  // the graph's grids change: drop it once no launch is in flight
+        const int rc = check_cuda(cudaDeviceSynchronize());
+        if (rc != CMF_OK) return rc;
+    }
+    destroy_graph(p);
+    const CmfView& v = p->view;
+    const long per_block = (long)p->tpb * width;
+    p->mtile = width;
+    p->cell_blocks = ceil_div((long)v.num_catchments * M, per_block);
+    p->path_blocks = (v.features & CMF_FEAT_BIFURCATION)
+                         ? ceil_div((long)v.num_bifurcation_paths * M, per_block) : 0;
+    p->levee_blocks = (v.features & CMF_FEAT_LEVEE) ? ceil_div((long)v.num_levees * M, per_block) : 0;
+    Layout L = layout_of(&v, p->layout_blocks);
+    if (p->fp64) fill_dev<double>(p, L, true);
+    else fill_dev<float>(p, L, true);
+    return CMF_OK;
 }
 
 int cmf_stats_attach(CmfPlan* p, int count, const CmfStatistic* stats, double* weight)
@@ -950,6 +979,7 @@ extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
     p.one = true;
     p.tpb = block_of(&v);
     p.cell_blocks = ceil_div((long)v.num_catchments, p.tpb);
+    p.layout_blocks = p.cell_blocks;
     p.path_blocks = (f & CMF_FEAT_BIFURCATION) ? ceil_div((long)v.num_bifurcation_paths, p.tpb) : 0;
     p.levee_blocks = (f & CMF_FEAT_LEVEE) ? ceil_div((long)v.num_levees, p.tpb) : 0;
     const bool res = f & CMF_FEAT_RESERVOIR, lev = f & CMF_FEAT_LEVEE,

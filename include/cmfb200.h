@@ -220,6 +220,13 @@ int cmf_workspace_size(const CmfView* view, size_t* bytes);
  * that changes those parameters afterwards creates a new plan. */
 int cmf_plan_create(const CmfView* view, CmfPlan** plan);
 void cmf_plan_destroy(CmfPlan* plan);
+/* Member-tile width of the member-batched kernels (no counterpart in the
+ * reference): each thread handles `width` consecutive members of one
+ * catchment, so the catchment's shared fields are loaded once from HBM and
+ * then from L1.  width divides num_members (1 for one member); the default is
+ * 1, and the interval graph is rebuilt on the next step.  The autotuner picks
+ * it with the block size. */
+int cmf_plan_set_member_tile(CmfPlan* plan, int32_t width);
 
 /* ---- the step path ------------------------------------------------------- */
 /* Advance one forcing interval of `outer_seconds`.  Replaces the body of

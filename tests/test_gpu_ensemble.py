@@ -87,3 +87,42 @@ def test_full_physics_members_equal_plain_runs(batched, device):
             np.testing.assert_array_equal(a[k][..., m].cpu().numpy(), b[k].cpu().numpy(),
                                           err_msg=f"member {m} field {k}")
     ens.check_status()
+
+
+@pytest.mark.parametrize("width", [2, 4])
+def test_member_tile_changes_no_result(width, device):
+    """A thread per W consecutive members of a cell (cmf_plan_set_member_tile)
+    routes exactly as a thread per member: levees, bifurcation paths and
+    reservoirs, members with their own Manning and runoff, the tile switched
+    between days."""
+    members = 8
+    net = syn.generate(syn.NetworkSpec(20_000, seed=29, bifurcation_paths=150, levee_fraction=0.25,
+                                       reservoirs=12))
+    n = net.num_catchments
+    rfac, mfac = syn.ensemble_factors(n, members, seed=29)
+    per = {"river_manning": (net.fields["river_manning"][:, None] * mfac).astype(np.float32)}
+    kw = dict(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+              num_members=members, batched_fields=per)
+    ref, tiled = CaMaFlood(**kw), CaMaFlood(**kw)
+    tiled.set_member_tile(width)
+    order = ref.order
+    for day in range(3):
+        r = syn.daily_runoff(net, day)
+        rm = torch.as_tensor((r[:, None] * rfac).astype(np.float32)[order]).to(device)
+        for m in (ref, tiled):
+            m.set_inputs(rm)
+            m.step_advance()
+        if day == 1:
+            tiled.set_member_tile(1)
+            tiled.set_member_tile(width)
+        torch.cuda.synchronize()
+        a, b = ref.state_tensors(), tiled.state_tensors()
+        for k in a:
+            np.testing.assert_array_equal(b[k].cpu().numpy(), a[k].cpu().numpy(),
+                                          err_msg=f"day {day} field {k}")
+    assert tiled.member_tile == width
+    tiled._rebuild_plan(128)                  # a rebuilt plan keeps the tile
+    assert tiled.member_tile == width
+    with pytest.raises(ValueError):
+        tiled.set_member_tile(3)
+    tiled.check_status()
