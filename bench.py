@@ -266,7 +266,7 @@ def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: flo
 
 
 def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
-                     member_tile: int = 2, block: int = 128) -> dict:
+                     member_tile: int = 16, block: int = 64) -> dict:
     """The batched-ensemble workload: `members` members of a `basins`-basin
     network (~`catchments` catchments per member, 6M by default; runoff and
     river Manning perturbed per member, daily forcing, per-member dt).  One
@@ -830,11 +830,11 @@ def main() -> None:
     ap.add_argument("--ensemble-catchments", type=int, default=6_000_000,
                     help="catchments per member of that comparison (the benchmark's ensemble "
                          "workload: ~6M in 500 basins)")
-    ap.add_argument("--ensemble-member-tile", type=int, default=2,
+    ap.add_argument("--ensemble-member-tile", type=int, default=16,
                     help="members of a catchment per thread in the batched model "
-                         "(0: autotuned block size and tile); 2 with 128-thread CTAs is "
+                         "(0: autotuned block size and tile); 16 with 64-thread CTAs is "
                          "the fastest pair measured at 64 members x 6M catchments")
-    ap.add_argument("--ensemble-block", type=int, default=128,
+    ap.add_argument("--ensemble-block", type=int, default=64,
                     help="threads per CTA of the batched model")
     args = ap.parse_args()
     if args.warmup < 3:

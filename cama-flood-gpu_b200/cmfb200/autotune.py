@@ -25,7 +25,7 @@ import torch
 from . import _lib
 
 DEFAULT_CANDIDATES = (64, 128, 192, 256)
-DEFAULT_TILES = (1, 2, 4, 8)
+DEFAULT_TILES = (1, 2, 4, 8, 16)
 _PARTS = (_lib.PART_MOMENTUM, _lib.PART_LIMIT, _lib.PART_STAGE, _lib.PART_LEVEE)
 
 

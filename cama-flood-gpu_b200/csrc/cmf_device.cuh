@@ -130,11 +130,21 @@ struct Dev {
 template <bool ONE>
 __device__ __forceinline__ long ix(long i, int m, int M) { return ONE ? i : i * (long)M + m; }
 
-// Member-tile width of the batched kernels (1 for one member): thread t0
-// handles elements t0 * W .. t0 * W + W - 1 of the member-innermost order,
-// W consecutive members of one cell, whose cell-shared loads then hit L1.
+// Member-tile width of the batched kernels (1 for one member).  Warp g owns
+// the 32 * W consecutive elements [32 W g, 32 W (g + 1)) of the member-
+// innermost order and walks them in W warp-wide rows: lane l of the warp
+// takes elements 32 W g + 32 w + l, w = 0 .. W-1.  Every row is a coalesced
+// run of 32 members, and with 32 W <= M all W rows of a warp belong to one
+// cell, whose topology and static fields the warp then reads once per row
+// from L1.  Elements grow with w, so past the end in one row means past the
+// end in all later rows.
 template <typename REAL, bool ONE>
 __device__ __forceinline__ int mtile_of(const Dev<REAL>& v) { return ONE ? 1 : v.mtile; }
+
+__device__ __forceinline__ long tile_elem(long t0, int w, int W)
+{
+    return ((t0 >> 5) * W + w) * 32 + (t0 & 31);
+}
 
 // (item, member) of flat thread index t over [items, M]: a shift and a mask
 // when M is a power of two, a division otherwise.
@@ -518,7 +528,7 @@ __global__ void __launch_bounds__(256, CMF_MOMENTUM_MIN_BLOCKS(REAL, ONE)) k_mom
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
         const long t0 = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
         for (int w = 0; w < W; ++w) {
-            const long t = t0 * W + w;
+            const long t = tile_elem(t0, w, W);
             if (t >= v.P * (long)v.M) return;
             int m;
             long p = split_member<ONE>(v, t, m);
@@ -528,7 +538,7 @@ __global__ void __launch_bounds__(256, CMF_MOMENTUM_MIN_BLOCKS(REAL, ONE)) k_mom
     }
     const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
     for (int w = 0; w < W; ++w) {
-        const long t = t0 * W + w;
+        const long t = tile_elem(t0, w, W);
         if (t >= v.N * (long)v.M) return;
         int m;
         long i = split_member<ONE>(v, t, m);
@@ -1077,7 +1087,7 @@ __global__ void __launch_bounds__(256, (sizeof(REAL) == 4 ? 8 : 4)) k_limit(cons
     const int W = mtile_of<REAL, ONE>(v);
     const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
     for (int w = 0; w < W; ++w) {
-        const long t = t0 * W + w;
+        const long t = tile_elem(t0, w, W);
         if (t >= v.N * (long)v.M) return;
         int m;
         long i = split_member<ONE>(v, t, m);
@@ -1122,7 +1132,7 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
     const int W = mtile_of<REAL, ONE>(v);
     const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
     for (int w = 0; w < W; ++w) {
-        const long t = t0 * W + w;
+        const long t = tile_elem(t0, w, W);
         if (t >= v.NLV * (long)v.M) break;
         int m;
         const long li = split_member<ONE>(v, t, m);
@@ -1184,7 +1194,7 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
     if (BIF && (int)blockIdx.x >= v.cell_blocks) {
         const long t0 = (long)(blockIdx.x - v.cell_blocks) * blockDim.x + threadIdx.x;
         for (int w = 0; w < W; ++w) {
-            const long t = t0 * W + w;
+            const long t = tile_elem(t0, w, W);
             if (t >= v.P * (long)v.M) break;
             int m;
             long p = split_member<ONE>(v, t, m);
@@ -1196,7 +1206,7 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
         for (int q = 0; q < kBudgetTerms; ++q) bud[q] = 0.0;
         const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
         for (int w = 0; w < W; ++w) {
-            const long t = t0 * W + w;
+            const long t = tile_elem(t0, w, W);
             if (t >= v.N * (long)v.M) break;
             int m;
             long i = split_member<ONE>(v, t, m);
