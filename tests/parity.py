@@ -122,3 +122,36 @@ def mismatch_fraction(model: CaMaFlood, orc: O.Oracle, rtol: float = 1e-5) -> di
         floor = max(1e-3 * float(np.mean(np.abs(r))), 1e-30)
         out[k] = float(np.mean(np.abs(a - r) > rtol * (np.abs(r) + floor)))
     return out
+
+
+def ref_cuda_from_oracle(net: syn.Network, orc: O.Oracle):
+    """The reference's CUDA kernels (oracle/_ref) loaded with the oracle's
+    current state."""
+    from oracle import ref_cuda as RC
+    f = O.reference_fields(net.fields, net.opened_modules)
+    st = orc.state()
+    f.update({k: st[k] for k in CELL_REAL + CELL_STO})
+    if "bifurcation" in net.opened_modules:
+        f.update({k: st[k] for k in PATH_FIELDS})
+    if "reservoir" in net.opened_modules:
+        f["reservoir_total_inflow"] = st["reservoir_total_inflow"]
+    return RC.RefCuda(f, net.opened_modules)
+
+
+def assert_bit_exact(model: CaMaFlood, ref_state: dict, diag: bool) -> None:
+    """Every state field of the model equals the reference CUDA state."""
+    order = model.order
+    for k in CELL_REAL + CELL_STO:
+        np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(), ref_state[k][order],
+                                      err_msg=k)
+    if model.bifurcation is not None:
+        for k in PATH_FIELDS:
+            np.testing.assert_array_equal(getattr(model.bifurcation, k).cpu().numpy(),
+                                          ref_state[k], err_msg=k)
+    if model.reservoir is not None:
+        np.testing.assert_array_equal(model.reservoir.reservoir_total_inflow.cpu().numpy(),
+                                      ref_state["reservoir_total_inflow"][order])
+    if diag:
+        for k in ("river_inflow", "flood_inflow"):
+            np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(),
+                                          ref_state[k][order], err_msg=k)

@@ -20,7 +20,7 @@ import pytest
 import torch
 
 from cmfb200 import synthetic as syn
-from oracle import oracle as O, ref_cuda as RC
+from oracle import ref_cuda as RC
 
 import parity as P
 
@@ -55,33 +55,8 @@ def _single_substep(case, precision="float32", n=6000):
     return model, orc
 
 
-def _ref_from_oracle(net, orc):
-    f = O.reference_fields(net.fields, net.opened_modules)
-    st = orc.state()
-    f.update({k: st[k] for k in P.CELL_REAL + P.CELL_STO})
-    if "bifurcation" in net.opened_modules:
-        f.update({k: st[k] for k in P.PATH_FIELDS})
-    if "reservoir" in net.opened_modules:
-        f["reservoir_total_inflow"] = st["reservoir_total_inflow"]
-    return RC.RefCuda(f, net.opened_modules)
-
-
-def _assert_bit_exact(model, ref_state, diag: bool):
-    order = model.order
-    for k in P.CELL_REAL + P.CELL_STO:
-        np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(), ref_state[k][order],
-                                      err_msg=k)
-    if model.bifurcation is not None:
-        for k in P.PATH_FIELDS:
-            np.testing.assert_array_equal(getattr(model.bifurcation, k).cpu().numpy(),
-                                          ref_state[k], err_msg=k)
-    if model.reservoir is not None:
-        np.testing.assert_array_equal(model.reservoir.reservoir_total_inflow.cpu().numpy(),
-                                      ref_state["reservoir_total_inflow"][order])
-    if diag:
-        for k in ("river_inflow", "flood_inflow"):
-            np.testing.assert_array_equal(getattr(model.base, k).cpu().numpy(),
-                                          ref_state[k][order], err_msg=k)
+_ref_from_oracle = P.ref_cuda_from_oracle
+_assert_bit_exact = P.assert_bit_exact
 
 
 @needs_ref
