@@ -110,7 +110,8 @@ def tune_block_size(model, candidates: Iterable[int] = DEFAULT_CANDIDATES, sub_s
     best_b, best_w = min(times, key=times.get)
     model._rebuild_plan(best_b)
     model.set_member_tile(best_w)
-    torch.cuda.synchronize(model.device)
+    if torch.device(model.device).type == "cuda":
+        torch.cuda.synchronize(model.device)
     shown = ({b: t for (b, _), t in times.items()} if tiles == [1]
              else {f"{b}/{w}": t for (b, w), t in times.items()})
     if cache_path:
