@@ -58,6 +58,30 @@ def algorithmic_bytes(n: int, n_paths: int, n_levees: int, n_res: int, full: boo
     return b
 
 
+def fp64_algorithmic_bytes(n: int, n_paths: int, n_levees: int, n_res: int) -> float:
+    """The full-physics rule of algorithmic_bytes with every REAL field in fp64
+    (the adjoint's primal): per catchment the downstream index 4 + 8 parameters
+    x 8 + flood table 80 + runoff 8 + state read 72 + state write 80 = 308, plus
+    protected storage 16 + protected depth 16 + masks 3; 28 per levee; per
+    bifurcation path 8 + 8 + 5 levels x (24 read + 32 read/write) = 296; 72 per
+    reservoir."""
+    return 343.0 * n + 28.0 * n_levees + 296.0 * n_paths + 72.0 * n_res
+
+
+def adjoint_algorithmic_bytes(n: int, n_paths: int, n_levees: int, n_res: int, state_len: int,
+                              slot_len: int, n_grad: int) -> float:
+    """Compulsory bytes of one sub-step of forward+adjoint with checkpoints:
+    the primal twice (the checkpointed forward and the taped recompute), the
+    tape slot written once and read once, the parameters read by the reverse
+    sweep (fp64: 148 per catchment, 28 per levee, 136 per path, 56 per
+    reservoir), the adjoint state read and written (state_len doubles), and
+    n_grad per-catchment parameter gradients accumulated (read and write)."""
+    fwd = fp64_algorithmic_bytes(n, n_paths, n_levees, n_res)
+    params = 148.0 * n + 28.0 * n_levees + 136.0 * n_paths + 56.0 * n_res
+    return (2.0 * fwd + 2.0 * 8.0 * slot_len + params + 2.0 * 8.0 * state_len
+            + 16.0 * n_grad * n)
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -443,9 +467,21 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
                                       params["river_height"], params["river_width"], forcing,
                                       state0, keep_checkpoints=False)
     subs = int(sum(counts))
+    n_lev = model.levee.num_levees if model.levee is not None else 0
+    n_res = model.reservoir.num_reservoirs if model.reservoir is not None else 0
     model.close()
     n = eng.N
+    peak, peak_kind = measured_peak()
+    b_fwd = fp64_algorithmic_bytes(n, eng.P, n_lev, n_res)
+    b_adj = adjoint_algorithmic_bytes(n, eng.P, n_lev, n_res, eng.state_len, eng.slot_len,
+                                      eng.n_grad)
+    ach_fwd = b_fwd * subs / t_fwd / 1e9
+    ach_adj = b_adj * subs / t_adj / 1e9
     return {"fwd_value": n * subs / t_fwd, "fwd_adj_value": n * subs / t_adj, "unit": UNIT,
+            "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+                         "fwd_bytes_per_substep": b_fwd, "fwd_adj_bytes_per_substep": b_adj,
+                         "fwd_achieved": ach_fwd, "fwd_frac": ach_fwd / peak,
+                         "fwd_adj_achieved": ach_adj, "fwd_adj_frac": ach_adj / peak},
             "fwd_adj_over_fwd": t_adj / t_fwd,
             "repeats": reps, "fwd_adj_over_fwd_each": [a / f for a, f in zip(ta, tf)],
             "product_fwd_value": n * subs / t_prod, "fwd_adj_over_product_fwd": t_adj / t_prod,
