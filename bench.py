@@ -364,7 +364,19 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
     plain.close()
     batched = n * n_batched / t_batched
     looped = n * n_looped / t_looped
-    return {"value": batched, "looped_value": looped, "speedup": batched / looped,
+    # algorithmic bytes (plain physics): a looped cell-sub-step moves the
+    # 172 B of algorithmic_bytes; a batched member-cell-sub-step moves its own
+    # state, runoff and river Manning (44 + 48 + 4 + 4 = 100 B) and a 1/M
+    # share of the other, shared parameters (72 B)
+    b_batched = 100.0 + 72.0 / members
+    b_looped = algorithmic_bytes(1, 0, 0, 0, False)
+    peak, peak_kind = measured_peak()
+    roof = {"bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+            "batched_bytes_per_member_substep": b_batched, "looped_bytes_per_substep": b_looped,
+            "batched_achieved": b_batched * batched / 1e9,
+            "batched_frac": b_batched * batched / 1e9 / peak,
+            "looped_achieved": b_looped * looped / 1e9, "looped_frac": b_looped * looped / 1e9 / peak}
+    return {"value": batched, "looped_value": looped, "speedup": batched / looped, "roofline": roof,
             "unit": UNIT, "members": members, "catchments_per_member": n, "basins": basins,
             "member_tile": tile, "block": block,
             "sub_steps_per_member_mean": n_batched / members,
