@@ -16,8 +16,6 @@ of every catchment contiguous), its flags and sparse slot tables.
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 

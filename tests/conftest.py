@@ -4,7 +4,6 @@ CPU tests (-m "not gpu") exercise the oracle against golden vectors, the host
 topology/index code and the C-ABI surface of libcmfb200 without launching any
 kernel.  GPU tests (-m gpu) compare the CUDA path with the oracle.
 """
-import os
 import sys
 from pathlib import Path
 

@@ -2,9 +2,6 @@
 symbol, and the ctypes view layout matches the C struct field by field."""
 import ctypes
 
-import numpy as np
-import pytest
-
 from cmfb200 import _lib
 
 

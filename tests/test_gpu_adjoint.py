@@ -12,7 +12,7 @@ import pytest
 import torch
 
 from cmfb200 import CaMaFlood, synthetic as syn, topology
-from cmfb200.adjoint import AdjointRouting, CELL_STATE, PARAMS
+from cmfb200.adjoint import AdjointRouting, PARAMS
 from oracle import step_torch as ST
 
 pytestmark = pytest.mark.gpu
