@@ -126,3 +126,41 @@ def test_member_tile_changes_no_result(width, device):
     with pytest.raises(ValueError):
         tiled.set_member_tile(3)
     tiled.check_status()
+
+
+@pytest.mark.parametrize("width", [1, 2])
+def test_fp64_full_physics_members_equal_plain_runs(width, device):
+    """The fp64 kernels (precision="float64") batched over members, with and
+    without a member tile, against plain fp64 runs of each member."""
+    members = 4
+    net = syn.generate(syn.NetworkSpec(8_000, seed=37, bifurcation_paths=80, levee_fraction=0.25,
+                                       reservoirs=8))
+    n = net.num_catchments
+    rfac, mfac = syn.ensemble_factors(n, members, seed=37)
+    manning = (net.fields["river_manning"][:, None] * mfac).astype(np.float64)
+    ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+                    num_members=members, batched_fields={"river_manning": manning},
+                    precision="float64")
+    ens.set_member_tile(width)
+    plains = []
+    for m in range(members):
+        f = dict(net.fields)
+        f["river_manning"] = np.ascontiguousarray(manning[:, m])
+        plains.append(CaMaFlood(device=device, input_proxy=f, opened_modules=net.opened_modules,
+                                precision="float64"))
+    order = ens.order
+    for day in range(2):
+        rm = (syn.daily_runoff(net, day)[:, None] * rfac)[order]
+        ens.set_inputs(torch.as_tensor(rm, dtype=torch.float64).to(device))
+        ens.step_advance()
+        for m, p in enumerate(plains):
+            p.set_inputs(torch.as_tensor(np.ascontiguousarray(rm[:, m]), dtype=torch.float64).to(device))
+            p.step_advance()
+    torch.cuda.synchronize()
+    a = ens.state_tensors()
+    for m, p in enumerate(plains):
+        b = p.state_tensors()
+        for k in b:
+            np.testing.assert_array_equal(a[k][..., m].cpu().numpy(), b[k].cpu().numpy(),
+                                          err_msg=f"member {m} field {k}")
+    ens.check_status()
