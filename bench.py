@@ -182,6 +182,19 @@ def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15
     for _ in range(reps):
         orc.substep()
     dt = time.perf_counter() - t0
+    # the same port on one core, a shorter sample (about a third of the time)
+    O.set_threads(1)
+    try:
+        t0 = time.perf_counter()
+        orc.substep()
+        one1 = time.perf_counter() - t0
+        reps1 = max(1, min(200, int(target_seconds / 3.0 / max(one1, 1e-6))))
+        t0 = time.perf_counter()
+        for _ in range(reps1):
+            orc.substep()
+        dt1 = time.perf_counter() - t0
+    finally:
+        O.set_threads(threads)
     return {
         "value": net.num_catchments * reps / dt,
         "unit": UNIT,
@@ -189,6 +202,8 @@ def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15
         "kind": "port",
         "sample": f"{reps} sub-steps of the {net.num_catchments}-catchment network "
                   f"(oracle/cmf_oracle.c, OpenMP, {threads} threads), dt={cfg['interval'] / max(n, 1):.1f}s",
+        "value_1_core": net.num_catchments * reps1 / dt1,
+        "sample_1_core": f"{reps1} sub-steps, 1 thread",
     }
 
 
