@@ -22,6 +22,10 @@
 // After them, with output statistics attached, k_stats_accumulate folds the
 // sub-step into the statistics.
 //
+// With several members the state is member-innermost ([N][M]) and a thread
+// of the per-catchment, per-path and per-levee parts walks W elements of that
+// order (the member tile, see tile_elem); W = 1 for one member.
+//
 // Catchments are stored breadth-first from the mouths, so the upstream cells
 // of p are [up[p], up[p+1]) and no upstream index array exists.  Every float
 // expression keeps the operand order of the reference kernels it replaces so
