@@ -665,6 +665,47 @@ class CaMaFlood:
         """limiter + inflow + bifurcation inflow + storage/flood/levee stage."""
         _lib.check(_lib.lib().cmf_phase_stage(self._plan, self._stream(), int(diag)), "phase_stage")
 
+    # The reference's phase callables, in the order of its sub-step loop
+    # (cmfgpu/models/cama_flood_model.py:134-162).  The kernels here fuse
+    # several phases: the first callable of each fused group launches the
+    # group and the others are no-ops, so that loop runs unchanged on this
+    # model.  The groups are:
+    #   compute_outflow        outflow, reservoir release, (levee) bifurcation outflow
+    #   compute_flood_stage    inflow and limiter, bifurcation inflow, flood stage, levee stage
+    # The inflow diagnostics (river_inflow, flood_inflow) are therefore written
+    # by compute_flood_stage, not by compute_inflow.
+    def compute_outflow(self) -> None:
+        self.compute_momentum(diag=True)
+
+    def compute_reservoir_outflow(self) -> None:
+        """Part of compute_outflow."""
+
+    def compute_bifurcation_outflow(self) -> None:
+        """Part of compute_outflow."""
+
+    def compute_levee_bifurcation_outflow(self) -> None:
+        """Part of compute_outflow."""
+
+    def compute_inflow(self) -> None:
+        """Part of compute_flood_stage (the inflow is gathered there)."""
+
+    def compute_bifurcation_inflow(self) -> None:
+        """Part of compute_flood_stage."""
+
+    def compute_flood_stage(self) -> None:
+        self.compute_stage(diag=True)
+
+    def compute_flood_stage_log(self) -> None:
+        """compute_flood_stage; the water budget accumulates when the model
+        was built with the log module."""
+        self.compute_stage(diag=True)
+
+    def compute_levee_stage(self) -> None:
+        """Part of compute_flood_stage."""
+
+    def compute_levee_stage_log(self) -> None:
+        """Part of compute_flood_stage."""
+
     def launch_substep_kernel(self, k: int, part: int) -> None:
         """Launch one kernel of sub-step k directly (for per-kernel timing)."""
         _lib.check(_lib.lib().cmf_launch_substep(self._plan, self._stream(), int(k), int(part)),

@@ -97,6 +97,43 @@ def test_interval_bit_exact_vs_reference_cuda(case, device):
     _assert_bit_exact(model, ref.state(), diag=True)
 
 
+@needs_ref
+@pytest.mark.parametrize("case", ["full", "res"])
+def test_reference_phase_sequence_bit_exact(case, device):
+    """One sub-step driven by the reference's own phase loop
+    (cama_flood_model.py:134-162) through the model's phase callables."""
+    net, orc = _spun_up(case)
+    ref = _ref_from_oracle(net, orc)
+    model = P.model_for(net)
+    P.load_oracle_state(model, orc)
+    r = syn.daily_runoff(net, 6)
+    ref.set_runoff(r)
+    model.set_inputs(torch.as_tensor(r[model.order]).cuda())
+    model.compute_adaptive_time_step()
+    n = ref.adaptive_sub_steps(86400.0)
+    ref.t["time_step"].fill_(86400.0 / n)
+    assert int(model.sub_step_counts()[0].item()) == n
+    ref.substep()
+    bif, lev, res = (model.bifurcation is not None, model.levee is not None,
+                     model.reservoir is not None)
+    model.compute_outflow()
+    if res:
+        model.compute_reservoir_outflow()
+    if bif:
+        if lev:
+            model.compute_levee_bifurcation_outflow()
+        else:
+            model.compute_bifurcation_outflow()
+    model.compute_inflow()
+    if bif:
+        model.compute_bifurcation_inflow()
+    model.compute_flood_stage()
+    if lev:
+        model.compute_levee_stage()
+    torch.cuda.synchronize()
+    _assert_bit_exact(model, ref.state(), diag=True)
+
+
 @pytest.mark.parametrize("case", list(P.CASES))
 def test_single_substep_matches_oracle(case, device):
     model, orc = _single_substep(case)
