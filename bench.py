@@ -135,33 +135,96 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def build_workload(name: str, seed_offset: int):
+def build_workload(name: str, seed_offset: int, topo=None):
+    """The seeded network of workload `name`; `topo` replaces the product's
+    integration helpers (the reference arm passes the oracle's, so that it
+    never loads libcmfb200)."""
     from cmfb200 import synthetic as syn
     cfg = dict(syn.CONFIGS[name])
     spec = cfg["spec"]
     spec = syn.NetworkSpec(**{**spec.__dict__, "seed": spec.seed + seed_offset})
-    net = syn.generate(spec)
+    net = syn.generate(spec, topo=topo)
     return net, cfg
 
 
-def runoff_series(net, cfg, count: int) -> np.ndarray:
-    """Forcing of `count` consecutive intervals (input order), float32 m^3/s."""
+def intervals_per_day(cfg) -> int:
+    return max(1, int(round(86400.0 / cfg["interval"])))
+
+
+def runoff_series(net, cfg, count: int, start: int = 0) -> np.ndarray:
+    """Forcing of intervals start .. start+count-1 (input order), float32 m^3/s:
+    daily gamma runoff, split by a random diurnal profile for sub-daily
+    intervals."""
     from cmfb200 import synthetic as syn
     out = np.empty((count, net.num_catchments), dtype=np.float32)
     if cfg["interval"] >= 86400.0:
-        for k in range(count):
-            out[k] = syn.daily_runoff(net, k)
+        for j in range(count):
+            out[j] = syn.daily_runoff(net, start + j)
     else:
-        per_day = int(round(86400.0 / cfg["interval"]))
+        per_day = intervals_per_day(cfg)
         day = None
-        for k in range(count):
-            d, h = divmod(k, per_day)
+        for j in range(count):
+            d, h = divmod(start + j, per_day)
             if d != day:
                 daily = syn.daily_runoff(net, d)
                 prof = syn.diurnal_profile(d, seed=net.spec.seed, hours=per_day)
                 day = d
-            out[k] = daily * prof[h]
+            out[j] = daily * prof[h]
     return out
+
+
+def spin_up(net, cfg, days: int, device, order, set_runoff, advance) -> int:
+    """Route `days` simulated days (the first days*intervals_per_day intervals
+    of runoff_series, same values) before anything is timed, so that timing
+    sees a flooded, spun-up state instead of the cold start.  Daily runoff is
+    uploaded once per day and split on the device (float32 products, equal to
+    runoff_series').  `order` maps the caller's catchment order to input
+    order (None: input order).  Returns the intervals routed."""
+    import torch
+    from cmfb200 import synthetic as syn
+    per_day = intervals_per_day(cfg)
+    for d in range(days):
+        daily = syn.daily_runoff(net, d)
+        if order is not None:
+            daily = daily[order]
+        dev = torch.as_tensor(daily).to(device)
+        if cfg["interval"] >= 86400.0:
+            set_runoff(dev)
+            advance()
+            continue
+        prof = syn.diurnal_profile(d, seed=net.spec.seed, hours=per_day)
+        for h in range(per_day):
+            set_runoff(dev * float(prof[h]))
+            advance()
+    return days * (per_day if cfg["interval"] < 86400.0 else 1)
+
+
+def workload_config(args, net, cfg, world: int) -> dict:
+    """The `config` object of both arms (identical keys and values)."""
+    f = net.fields
+    return {"workload": args.workload, "catchments_per_gpu": net.num_catchments,
+            "bifurcation_paths": int(f["bifurcation_catchment_id"].shape[0])
+            if "bifurcation_catchment_id" in f else 0,
+            "levees": int(f["levee_catchment_id"].shape[0]) if "levee_catchment_id" in f else 0,
+            "reservoirs": int(f["reservoir_catchment_id"].shape[0])
+            if "reservoir_catchment_id" in f else 0,
+            "interval_s": cfg["interval"], "spinup_days": args.spinup_days,
+            "parallelism": f"basin-sharded x{world}" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (state ~1 GB)"}
+
+
+def loaded_native_libraries() -> list[str]:
+    """In-tree shared libraries mapped into this process."""
+    seen = []
+    try:
+        with open("/proc/self/maps") as fh:
+            for line in fh:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and str(ROOT) in path and path not in seen:
+                    seen.append(path)
+    except OSError:
+        pass
+    return [str(Path(p).relative_to(ROOT)) if p.startswith(str(ROOT)) else p for p in seen]
 
 
 def cpu_sample(net, cfg, model_dt_hint: float | None, target_seconds: float = 15.0):
@@ -305,16 +368,18 @@ def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: flo
 
 
 def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
-                     member_tile: int = 16, block: int = 64) -> dict:
+                     member_tile: int = 16, block: int = 64, days: int = 5) -> dict:
     """The batched-ensemble workload: `members` members of a `basins`-basin
     network (~`catchments` catchments per member, 6M by default; runoff and
-    river Manning perturbed per member, daily forcing, per-member dt).  One
-    simulated day of the 30-day window (a bounded sample) in a single
-    member-innermost model (one launch per phase) against the same members run
-    one after another as plain models, both from the same initial state on the
-    same GPU.  The batched model runs `member_tile` members of a catchment per
-    thread in CTAs of `block` threads (member_tile 0: the autotuner picks both
-    on the first day); the looped plain models keep their default CTA size."""
+    river Manning perturbed per member, daily forcing, per-member dt).  The
+    first `days` simulated days of the 30-day window (a bounded sample) in a
+    single member-innermost model (one launch per phase) against the same
+    members run one after another as plain models over the same days, both
+    from the same initial state on the same GPU.  The batched model runs
+    `member_tile` members of a catchment per thread in CTAs of `block` threads
+    (member_tile 0: the autotuner picks both on the first day); the looped
+    plain models keep their default CTA size.  Forcing of every day and member
+    is resident on the device before timing."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn
     net = syn.generate_basins(basins, catchments, seed=3)
@@ -326,8 +391,9 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
                     num_members=members, batched_fields={"river_manning": manning},
                     **({"BLOCK_SIZE": block} if member_tile > 0 else {}))
     order = ens.order
-    rm = (syn.daily_runoff(net, 0)[:, None] * rfac).astype(np.float32)[order]
-    forcing = torch.as_tensor(rm).to(device)
+    rfac_dev = torch.as_tensor(np.ascontiguousarray(rfac[order])).to(device)
+    daily = torch.stack([torch.as_tensor(syn.daily_runoff(net, d)[order]) for d in range(days)]).to(device)
+    forcing = daily[:, :, None] * rfac_dev[None]               # [D, N, M] float32
     init = {k: v.clone() for k, v in ens.state_tensors().items()}
     stream = torch.cuda.current_stream(device)
 
@@ -335,7 +401,7 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
         for k, v in model.state_tensors().items():
             v.copy_(state[k])
 
-    ens.set_inputs(forcing)
+    ens.set_inputs(forcing[0])
     if member_tile > 0:
         ens.set_member_tile(member_tile)
     else:
@@ -344,39 +410,45 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
     reset(ens, init)
     torch.cuda.synchronize(device)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cnt_b = torch.zeros((days, members), dtype=torch.int32, device=device)
     a.record(stream)
-    ens.set_inputs(forcing)
-    ens.step_advance()
+    for d in range(days):
+        ens.set_inputs(forcing[d])
+        ens.step_advance()
+        cnt_b[d].copy_(ens.sub_step_counts())
     b.record(stream)
     torch.cuda.synchronize(device)
     t_batched = a.elapsed_time(b) / 1e3
-    n_batched = int(ens.sub_step_counts().sum().item())
+    n_batched = int(cnt_b.sum().item())
     tile, block = ens.member_tile, ens.block_size
     ens.close()
-    del ens, init
+    del ens, init, forcing
 
     plain = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=mods)
     init = {k: v.clone() for k, v in plain.state_tensors().items()}
     man_dev = torch.as_tensor(np.ascontiguousarray(manning[order].T)).to(device)
-    run_dev = torch.as_tensor(np.ascontiguousarray(rm.T)).to(device)
+    run_dev = (daily[None, :, :] * rfac_dev.T[:, None, :]).contiguous()   # [M, D, N]
     plain.base.river_manning.copy_(man_dev[0])
-    plain.set_inputs(run_dev[0])
+    plain.set_inputs(run_dev[0, 0])
     plain.step_advance()                    # graph build
     torch.cuda.synchronize(device)
-    n_looped = 0
     a.record(stream)
-    counts = torch.zeros(members, dtype=torch.int32, device=device)
+    cnt_l = torch.zeros((members, days), dtype=torch.int32, device=device)
     for m in range(members):
         reset(plain, init)
         plain.base.river_manning.copy_(man_dev[m])
-        plain.set_inputs(run_dev[m])
-        plain.step_advance()
-        counts[m].copy_(plain.sub_step_counts()[0])
+        for d in range(days):
+            plain.set_inputs(run_dev[m, d])
+            plain.step_advance()
+            cnt_l[m, d].copy_(plain.sub_step_counts()[0])
     b.record(stream)
     torch.cuda.synchronize(device)
     t_looped = a.elapsed_time(b) / 1e3
-    n_looped = int(counts.sum().item())
+    n_looped = int(cnt_l.sum().item())
+    same_counts = bool(torch.equal(cnt_b, cnt_l.T))
     plain.close()
+    del run_dev, daily, rfac_dev
+    torch.cuda.empty_cache()
     batched = n * n_batched / t_batched
     looped = n * n_looped / t_looped
     # algorithmic bytes (plain physics): a looped cell-sub-step moves the
@@ -393,23 +465,24 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
             "looped_achieved": b_looped * looped / 1e9, "looped_frac": b_looped * looped / 1e9 / peak}
     return {"value": batched, "looped_value": looped, "speedup": batched / looped, "roofline": roof,
             "unit": UNIT, "members": members, "catchments_per_member": n, "basins": basins,
-            "member_tile": tile, "block": block,
+            "member_tile": tile, "block": block, "days": days,
             "sub_steps_per_member_mean": n_batched / members,
-            "workload": "1 day (a sample of the 30-day window) of a member-innermost ensemble "
-                        "(runoff x lognormal(0.3), river Manning x U(0.8,1.2) per member) vs "
-                        "the members looped as plain models; includes the state reset copies "
-                        "of the looped runs"}
+            "same_sub_step_counts": same_counts,
+            "workload": f"{days} days (a sample of the 30-day window) of a member-innermost "
+                        "ensemble (runoff x lognormal(0.3), river Manning x U(0.8,1.2) per member) "
+                        "vs the members looped as plain models over the same days; includes the "
+                        "state reset copies of the looped runs"}
 
 
-def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
+def adjoint_compare(device, days: int, checkpoint_every: int = 96, repeats: int = 5) -> dict:
     """Forward+adjoint against forward on the calibration window: the
     250k-catchment full-physics network (8,000 bifurcation paths, levees on
     20 % of cells, 500 reservoirs), fp64, daily forcing over `days`
     intervals, discharge at 500 cells with upstream area > 1000 km^2,
     relative-misfit loss against a run with river Manning x lognormal(0.2).
     Both are timed with CUDA events on the same GPU from the same spun-up
-    state, three interleaved repetitions, medians; the gradient run includes
-    its checkpointed forward."""
+    state: one discarded warm-up pair, then `repeats` interleaved repetitions,
+    medians; the gradient run includes its checkpointed forward."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn, topology
     from cmfb200.adjoint import AdjointRouting
@@ -446,12 +519,13 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
         return torch.autograd.grad(loss, [p["river_manning"], p["river_height"],
                                           p["river_width"], f])
 
-    fwd()
-    fwd_adj()                                 # warm-up (allocations, lazy init)
+    for _ in range(2):                        # warm-up (allocations, lazy init, clocks)
+        fwd()
+        fwd_adj()
     torch.cuda.synchronize(device)
-    # three interleaved repetitions, medians reported (single runs vary by a
-    # few per cent with the GPU's power state)
-    reps = 3
+    # interleaved repetitions, medians reported (single runs vary by a few
+    # per cent with the GPU's power state)
+    reps = max(1, int(repeats))
     tf, ta = [], []
     for _ in range(reps):
         ev[0].record(stream)
@@ -489,6 +563,36 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
         torch.cuda.synchronize(device)
         tp.append(ev[0].elapsed_time(ev[1]) / 1e3)
     t_prod = statistics.median(tp)
+    # the product's mixed-precision forward (fp32 fluxes, fp64 storage: the
+    # reference's default) over the same window from the same state
+    mixed = CaMaFlood(device=device, input_proxy=net.fields,
+                      opened_modules=net.opened_modules, precision="float32")
+    for k, v in mixed.state_tensors().items():
+        v.copy_(snap[k].to(v.dtype))
+    mb = mixed.base
+    for k in ("river_manning", "flood_manning", "river_height", "river_width"):
+        getattr(mb, k).copy_(params[k].to(getattr(mb, k).dtype))
+    snap_m = {k: v.clone() for k, v in mixed.state_tensors().items()}
+    forcing32 = forcing.float()
+
+    def mixed_fwd():
+        for k, v in mixed.state_tensors().items():
+            v.copy_(snap_m[k])
+        for d in range(days):
+            mixed.set_inputs(forcing32[d])
+            mixed.step_advance()
+
+    mixed_fwd()
+    torch.cuda.synchronize(device)
+    tm = []
+    for _ in range(reps):
+        ev[0].record(stream)
+        mixed_fwd()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        tm.append(ev[0].elapsed_time(ev[1]) / 1e3)
+    t_mixed = statistics.median(tm)
+    mixed.close()
     # sub-step count of the window (the CFL counts of the primal run)
     _, _, counts, _, _ = eng._forward(params["river_manning"], params["flood_manning"],
                                       params["river_height"], params["river_width"], forcing,
@@ -504,21 +608,26 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96) -> dict:
                                       eng.n_grad)
     ach_fwd = b_fwd * subs / t_fwd / 1e9
     ach_adj = b_adj * subs / t_adj / 1e9
+    each = [a / f for a, f in zip(ta, tf)]
     return {"fwd_value": n * subs / t_fwd, "fwd_adj_value": n * subs / t_adj, "unit": UNIT,
             "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
                          "fwd_bytes_per_substep": b_fwd, "fwd_adj_bytes_per_substep": b_adj,
                          "fwd_achieved": ach_fwd, "fwd_frac": ach_fwd / peak,
                          "fwd_adj_achieved": ach_adj, "fwd_adj_frac": ach_adj / peak},
             "fwd_adj_over_fwd": t_adj / t_fwd,
-            "repeats": reps, "fwd_adj_over_fwd_each": [a / f for a, f in zip(ta, tf)],
+            "repeats": reps, "fwd_adj_over_fwd_each": each,
+            "fwd_adj_over_fwd_spread": (max(each) - min(each)) / statistics.median(each),
             "product_fwd_value": n * subs / t_prod, "fwd_adj_over_product_fwd": t_adj / t_prod,
+            "fwd_adj_over_mixed_product_fwd": t_adj / t_mixed,
+            "mixed_product_fwd_ms": t_mixed * 1e3,
             "catchments": n, "sub_steps": subs,
             "days": days, "checkpoint_every": checkpoint_every, "gauges": int(gauges.size),
             "dtype": "f64",
             "workload": "full-physics 250k network, fp64, daily forcing, gradients w.r.t. "
                         "river Manning, river height, river width and runoff; fwd = the same "
                         "primal kernels without checkpoints; product_fwd = CaMaFlood.step_advance "
-                        "in fp64 (interval graphs) over the same window"}
+                        "in fp64 (interval graphs) over the same window; mixed_product_fwd = the "
+                        "same in the reference's mixed precision (fp32 fluxes, fp64 storage)"}
 
 
 def adjoint_fd_check(device, days: int, cells: int, seed: int = 5) -> dict:
@@ -587,17 +696,110 @@ def adjoint_fd_check(device, days: int, cells: int, seed: int = 5) -> dict:
             worst = max(worst, err)
     model.close()
     return {"cells_per_field": cells, "fields": list(PARAMS) + ["runoff"], "passed": passed,
-            "total": total, "passed_at_h_1e-6": at_small_h, "max_scaled_error": worst,
+            "total": total, "passed_without_retry": passed - at_small_h,
+            "passed_at_h_1e-6": at_small_h, "max_scaled_error": worst,
             "days": days, "catchments": eng.N}
 
 
+REF_PHASES = ("outflow", "reservoir", "bif_outflow", "inflow", "bif_inflow", "flood_stage",
+              "levee_stage")
+
+
+def reference_cuda_measure(device, net, cfg, args, dev_forcing_in, our_state, order) -> dict:
+    """The reference's own CUDA kernels on the same workload and GPU: the
+    cmfgpu/phys/cuda/*.cu sources compiled unmodified for sm_100a
+    (oracle/_ref), driven as CaMaFlood.step_advance drives them
+    (cmfgpu/models/cama_flood_model.py:104-173): per interval the CFL kernel
+    and one .item() host sync, then per sub-step up to seven launches
+    (outflow, reservoir, bifurcation outflow, inflow, bifurcation inflow,
+    flood stage, levee stage) with fp64 atomic scatters.  It routes the same
+    spin-up and warm-up intervals and then the timed intervals from the same
+    initial state; its state after them is compared with ours field by
+    field."""
+    import torch
+    from oracle import oracle as O, ref_cuda as RC
+    if not RC.available():
+        return {"unavailable": "oracle/_ref (the reference CUDA kernels) is not built"}
+    fields = O.reference_fields(net.fields, net.opened_modules)
+    ref = RC.RefCuda(fields, net.opened_modules, device=device)
+    interval = cfg["interval"]
+    runoff = ref.t["runoff"]
+
+    def set_runoff(x):
+        runoff.copy_(x)
+
+    spin_up(net, cfg, args.spinup_days, device, None, set_runoff,
+            lambda: ref.step_advance(interval))
+    steps = dev_forcing_in.shape[0] - args.warmup
+    for k in range(args.warmup):
+        set_runoff(dev_forcing_in[k])
+        ref.step_advance(interval)
+    stream = torch.cuda.current_stream(device)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    subs = 0
+    e0.record(stream)
+    for k in range(args.warmup, args.warmup + steps):
+        set_runoff(dev_forcing_in[k])
+        subs += ref.step_advance(interval)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1)
+    # state after the same intervals: ours (model order) against the reference
+    mism = {}
+    for k, v in our_state.items():
+        r = ref.t[k]
+        a = v.cpu().numpy()
+        b = r.detach().cpu().numpy()
+        if a.ndim == 1:                       # catchment fields: input -> model order
+            b = b[order]
+        mism[k] = int(np.count_nonzero(a != b))
+    # per-kernel device times of one more interval (events around each launch)
+    mods = set(net.opened_modules)
+    set_runoff(dev_forcing_in[-1])
+    n = ref.adaptive_sub_steps(interval)
+    ref.t["time_step"].fill_(interval / n)
+    calls = [("outflow", ref.outflow, True), ("reservoir", ref.reservoir, "reservoir" in mods),
+             ("bif_outflow", ref.bif_outflow, "bifurcation" in mods),
+             ("inflow", ref.inflow, True), ("bif_inflow", ref.bif_inflow, "bifurcation" in mods),
+             ("flood_stage", ref.flood_stage, True), ("levee_stage", ref.levee_stage, "levee" in mods)]
+    calls = [(nm, fn) for nm, fn, on in calls if on]
+    evs = []
+    for _ in range(n):
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)]
+        marks[0].record(stream)
+        for j, (_, fn) in enumerate(calls):
+            fn()
+            marks[j + 1].record(stream)
+        evs.append(marks)
+    torch.cuda.synchronize(device)
+    per = {nm: float(np.mean([m[j].elapsed_time(m[j + 1]) for m in evs]))
+           for j, (nm, _) in enumerate(calls)}
+    value = net.num_catchments * subs / (ms / 1e3)
+    del ref
+    torch.cuda.empty_cache()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / steps, "sub_steps_timed": subs,
+            "ms_per_substep_kernels": per, "ms_per_substep_kernel_sum": sum(per.values()),
+            "launches_per_substep": len(calls),
+            "state_mismatches_vs_ours": mism,
+            "state_equal": all(v == 0 for v in mism.values()),
+            "what": "the reference's cmfgpu/phys/cuda kernels, unmodified, compiled for sm_100a "
+                    "(oracle/_ref), driven per interval as CaMaFlood.step_advance does (CFL kernel "
+                    "+ .item(), then up to 7 launches per sub-step, fp64 atomics), same intervals, "
+                    "same initial state, same GPU; device time by CUDA events"}
+
+
 def run_reference(args) -> None:
-    """CPU restatement of the reference path on all host cores (rank 0 only)."""
+    """The reference algorithm's CPU restatement on all host cores (rank 0
+    only).  The reference ships no CPU path, so this is the oracle port
+    (oracle/cmf_oracle.c, OpenMP).  The network is built with the oracle's
+    topology helpers and the product library is never loaded; the line lists
+    the in-tree libraries this process mapped."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import oracle as O
-    net, cfg = build_workload(args.workload, 0)
+    from oracle import oracle as O, topology as OT
+    net, cfg = build_workload(args.workload, 0, topo=OT)
     fields = O.reference_fields(net.fields, net.opened_modules)
     orc = O.Oracle(fields, net.opened_modules)
     threads = O.max_threads()
@@ -620,18 +822,21 @@ def run_reference(args) -> None:
             orc.substep()
     el = time.perf_counter() - t0
     value = net.num_catchments * per_step * args.steps / el
-    sample = (f"{per_step} of the interval's {n} sub-steps per step, "
+    sample = (f"{per_step} of the interval's {n} sub-steps per step from the cold start, "
               f"{net.num_catchments}-catchment {args.workload} network, {threads} OpenMP threads")
+    libs = loaded_native_libraries()
+    if any("libcmfb200" in x for x in libs):
+        raise RuntimeError(f"the reference arm loaded the product library: {libs}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": "synthetic (seeded generator)",
-        "config": {"workload": args.workload, "catchments": net.num_catchments,
-                   "interval_s": cfg["interval"]},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 flux / f64 storage",
+        "data": "synthetic (seeded generator, no CaMa maps)",
+        "config": workload_config(args, net, cfg, max(1, int(os.environ.get("WORLD_SIZE", "1")))),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "native_libraries": libs,
     }
     print(json.dumps(line), flush=True)
 
@@ -661,19 +866,26 @@ def run_ours(args) -> None:
     Lv = model.levee.num_levees if model.levee is not None else 0
     R = model.reservoir.num_reservoirs if model.reservoir is not None else 0
     total = args.warmup + args.steps
-    forcing = runoff_series(net, cfg, total)[:, model.order]          # model order
-    host = torch.from_numpy(forcing).pin_memory()
-    dev_forcing = host.to(device)
-    counts = torch.zeros(total, dtype=torch.int32, device=device)
+    order = model.order
+    order_dev = torch.as_tensor(order, device=device)
 
     def sync_all():
         torch.cuda.synchronize(device)
         if world > 1:
             dist.barrier()
 
+    # ---- spin-up: route the first simulated days (untimed, graphs) ------------
+    spun = spin_up(net, cfg, args.spinup_days, device, order, model.set_inputs,
+                   model.step_advance)
+    forcing_in = runoff_series(net, cfg, total, start=spun)           # input order
+    host = torch.from_numpy(np.ascontiguousarray(forcing_in[:, order])).pin_memory()
+    dev_forcing = host.to(device)                                      # model order
+    counts = torch.zeros(total, dtype=torch.int32, device=device)
+
     tuned = None
     if args.block == 0:
-        # block size chosen by the autotuner on this network (outside the timed region)
+        # block size chosen by the autotuner on this network (outside the timed
+        # region; the state is restored afterwards)
         model.set_inputs(dev_forcing[0])
         tuned = model.autotune_block_size()
 
@@ -715,6 +927,11 @@ def run_ours(args) -> None:
         dist.all_reduce(w, op=dist.ReduceOp.SUM)
     ms_max = float(t.item())
     value = float(w.item()) / (ms_max / 1e3)
+    # the state the timed intervals left, for the reference-CUDA comparison
+    our_state = {k: v.clone() for k, v in model.state_tensors().items()}
+    flooded = float((model.base.flood_storage > 0).double().mean().item())
+    prot = (float((model.base.protected_storage > 0).double().mean().item())
+            if model.levee is not None else 0.0)
 
     # ---- per-kernel timing (one interval through direct launches) -------------
     kern = {"momentum": [], "limit": [], "stage": [], "levee": []}
@@ -750,12 +967,14 @@ def run_ours(args) -> None:
     peak, peak_kind = measured_peak()
     achieved = alg / (t_sub / 1e3) / 1e9
     traffic = None
+    traffic_src = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
         try:
             tj = json.loads(tfile.read_text())
             if tj.get("workload") == args.workload:
                 traffic = tj.get("bytes_per_substep")
+                traffic_src = tj.get("source")
         except Exception:
             traffic = None
 
@@ -810,6 +1029,18 @@ def run_ours(args) -> None:
         forcing_leg = forcing_measure(device, net, model.base.catchment_id.cpu().numpy(),
                                       steps=args.forcing_steps)
 
+    ref_cuda = None
+    if world == 1 and args.reference_cuda:
+        model.close()
+        del dev_forcing
+        dev_in = torch.as_tensor(forcing_in).to(device)
+        ref_cuda = reference_cuda_measure(device, net, cfg, args, dev_in, our_state, order)
+        del dev_in
+        if "value" in ref_cuda:
+            ref_cuda["ours_over_reference_cuda"] = value / ref_cuda["value"]
+            ref_cuda["kernel_sum_ratio"] = ref_cuda["ms_per_substep_kernel_sum"] / t_sub
+    del our_state
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(net, cfg, None)
@@ -819,40 +1050,40 @@ def run_ours(args) -> None:
         model.close()
         ensemble = ensemble_compare(device, args.ensemble_members, args.ensemble_catchments,
                                     member_tile=args.ensemble_member_tile,
-                                    block=args.ensemble_block)
+                                    block=args.ensemble_block, days=args.ensemble_days)
 
     adjoint = None
     if world == 1 and args.adjoint_days > 0:
         model.close()
-        adjoint = adjoint_compare(device, args.adjoint_days)
+        adjoint = adjoint_compare(device, args.adjoint_days, repeats=args.adjoint_repeats)
         if args.adjoint_fd_cells > 0:
             adjoint["fd_check"] = adjoint_fd_check(device, args.adjoint_fd_days, args.adjoint_fd_cells)
 
     if world > 1:
         dist.barrier()
     if rank == 0:
+        config = workload_config(args, net, cfg, world)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 flux / f64 storage", "data": "synthetic (seeded generator, no CaMa maps)",
-            "config": {"workload": args.workload, "catchments_per_gpu": N,
-                       "bifurcation_paths": P, "levees": Lv, "reservoirs": R,
-                       "interval_s": cfg["interval"], "sub_steps_timed": substeps,
-                       "parallelism": f"basin-sharded x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (state ~1 GB)", "block": model.block_size,
-                       "block_tuned": tuned is not None},
+            "config": config,
+            "run": {"sub_steps_timed": substeps, "block": model.block_size,
+                    "block_tuned": tuned is not None, "spinup_intervals": spun,
+                    "flooded_cell_fraction": flooded, "protected_cell_fraction": prot},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 4,
                     "d2h_bytes_per_step": int(gauges.numel()) * 4,
                     "path": "InputPrefetcher.submit (pinned H2D on a copy stream) -> set_inputs -> "
                             "step_advance -> gauge D2H read by the host each interval",
                     "gauge_discharge_sum": gauge_sum},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                          "peak_kind": peak_kind, "kernel": "sub-step (k_momentum + k_limit + k_stage + k_levee)",
                          "algorithmic_bytes_per_substep": alg,
                          "ms_momentum": t_mom, "ms_limit": t_lim, "ms_stage": t_stage,
                          "ms_levee": t_lev},
+            "reference_cuda": ref_cuda,
             "cpu_baseline": cpu,
             "ensemble": ensemble,
             "adjoint": adjoint,
@@ -860,11 +1091,47 @@ def run_ours(args) -> None:
             "statistics": stats,
             "clocks": clocks,
             "gpu_launches": launches,
+            "native_libraries": loaded_native_libraries(),
         }
         print(json.dumps(line), flush=True)
     model.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def probe_kernels(args) -> None:
+    """One launch of each sub-step kernel on the spun-up workload, outside the
+    interval graph and inside an NVTX range named "probe", for a profiler to
+    capture (ncu --nvtx --nvtx-include "probe/").  Prints what it launched."""
+    import torch
+    from cmfb200 import CaMaFlood, _lib
+    device = torch.device("cuda", 0)
+    net, cfg = build_workload(args.workload, 0)
+    model = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+                      step_duration=cfg["interval"],
+                      max_sub_step_seconds=cfg.get("max_sub_step_seconds", 0.0),
+                      BLOCK_SIZE=args.block or 64)
+    spun = spin_up(net, cfg, args.spinup_days, device, model.order, model.set_inputs,
+                   model.step_advance)
+    model.set_inputs(torch.as_tensor(runoff_series(net, cfg, 1, start=spun)[0][model.order]).to(device))
+    model.compute_adaptive_time_step()
+    torch.cuda.synchronize(device)
+    parts = [("k_momentum", _lib.PART_MOMENTUM), ("k_limit", _lib.PART_LIMIT),
+             ("k_stage", _lib.PART_STAGE)]
+    if model.levee is not None:
+        parts.append(("k_levee", _lib.PART_LEVEE))
+    torch.cuda.nvtx.range_push("probe")
+    for _, part in parts:
+        model.launch_substep_kernel(0, part)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize(device)
+    model.check_status()
+    print(json.dumps({"probe": [p for p, _ in parts], "workload": args.workload,
+                      "catchments": net.num_catchments, "spinup_intervals": spun,
+                      "block": model.block_size,
+                      "flooded_cell_fraction": float((model.base.flood_storage > 0).double().mean().item())}),
+          flush=True)
+    model.close()
 
 
 def main() -> None:
@@ -881,7 +1148,9 @@ def main() -> None:
                     help="members of the batched-vs-looped comparison (0 skips it)")
     ap.add_argument("--adjoint-days", type=int, default=30,
                     help="daily intervals of the forward+adjoint comparison (0 = skip)")
-    ap.add_argument("--adjoint-fd-cells", type=int, default=0,
+    ap.add_argument("--adjoint-repeats", type=int, default=5,
+                    help="interleaved timed repetitions of the adjoint comparison")
+    ap.add_argument("--adjoint-fd-cells", type=int, default=50,
                     help="random cells per parameter of a finite-difference check of the "
                          "adjoint on the 250k network (0 = skip)")
     ap.add_argument("--adjoint-fd-days", type=int, default=3,
@@ -897,12 +1166,23 @@ def main() -> None:
                     help="members of a catchment per thread in the batched model "
                          "(0: autotuned block size and tile); 16 with 64-thread CTAs is "
                          "the fastest pair measured at 64 members x 6M catchments")
+    ap.add_argument("--ensemble-days", type=int, default=5,
+                    help="simulated days of the ensemble comparison")
+    ap.add_argument("--spinup-days", type=int, default=9,
+                    help="simulated days routed before the timed intervals (a warm, flooded state)")
+    ap.add_argument("--no-reference-cuda", dest="reference_cuda", action="store_false",
+                    help="skip timing the reference's own CUDA kernels on the same workload")
+    ap.add_argument("--probe-kernels", action="store_true",
+                    help="launch each sub-step kernel once on the spun-up workload inside an "
+                         "NVTX range 'probe' (for a profiler) and exit")
     ap.add_argument("--ensemble-block", type=int, default=64,
                     help="threads per CTA of the batched model")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.probe_kernels:
+        probe_kernels(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -77,7 +77,13 @@ class Network:
         return mods
 
 
-def generate(spec: NetworkSpec) -> Network:
+def generate(spec: NetworkSpec, topo=None) -> Network:
+    """The seeded network of `spec`.  `topo` supplies the three integration
+    helpers (accumulate_upstream, accumulate_downstream, init_river_depth);
+    the default is cmfb200.topology, which runs them in libcmfb200.  A
+    process that must not load the product library passes another module with
+    the same functions and gets the same network bit for bit."""
+    topo = topology if topo is None else topo
     rng = np.random.default_rng(spec.seed)
     n = int(spec.num_catchments)
     idx = np.arange(n, dtype=np.int64)
@@ -90,20 +96,20 @@ def generate(spec: NetworkSpec) -> Network:
 
     rivlen = (8000.0 * np.exp(0.5 * rng.standard_normal(n))).astype(np.float32)
     unit_area_km2 = rng.uniform(50.0, 500.0, size=n)
-    up_area_km2 = topology.accumulate_upstream(dn, unit_area_km2)
+    up_area_km2 = topo.accumulate_upstream(dn, unit_area_km2)
     rivwth = np.clip(0.4 * up_area_km2 ** 0.5, 10.0, 2000.0).astype(np.float32)
     rivhgt = np.clip(0.1 * up_area_km2 ** 0.3, 0.5, 15.0).astype(np.float32)
     slope = 1e-4 * np.exp(spec.slope_sigma * rng.standard_normal(n))
     drop = rivlen.astype(np.float64) * slope
     drop[mouth] = rng.uniform(0.0, 5.0, size=int(mouth.sum()))
-    elevation = topology.accumulate_downstream(dn, drop).astype(np.float32)
+    elevation = topo.accumulate_downstream(dn, drop).astype(np.float32)
     K = spec.num_flood_levels
     fldhgt = np.cumsum(rng.exponential(0.5, size=(n, K)), axis=1).astype(np.float32)
     nxtdst = rivlen.copy()
     nxtdst[mouth] = np.float32(10000.0)
     catchment_area = (unit_area_km2 * 1e6).astype(np.float32)
 
-    river_depth = topology.init_river_depth(elevation, rivhgt, dn)
+    river_depth = topo.init_river_depth(elevation, rivhgt, dn)
     river_storage = (rivlen * rivwth * river_depth).astype(np.float64)
 
     f: dict[str, np.ndarray] = {

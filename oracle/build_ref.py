@@ -2,8 +2,9 @@
 
     python oracle/build_ref.py
 
-Reads the reference sources where they lie (/root/reference/cmfgpu/phys/cuda,
-or $CMF_REFERENCE_ROOT) -- nothing is copied into this repository -- and
+Reads the reference sources where they lie (cmfgpu/phys/cuda under the
+checkout that oracle/refroot.py locates) -- nothing is copied into this
+repository -- and
 links them with oracle/ref_binding.cpp into oracle/_ref/cmf_refcuda*.so for
 sm_100a.  The output directory is git-ignored; the built module travels to the
 GPU box with the rest of the tree.  Skips (returns None) when the reference
@@ -11,13 +12,18 @@ tree is absent, e.g. on the GPU box, which only uses the prebuilt module.
 """
 from __future__ import annotations
 
-import os
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("CMF_REFERENCE_ROOT", "/root/reference")) / "cmfgpu" / "phys" / "cuda"
+try:
+    from .refroot import reference_root
+except ImportError:                      # run as a script
+    sys.path.insert(0, str(HERE))
+    from refroot import reference_root
+_ROOT = reference_root()
+REF = (_ROOT / "cmfgpu" / "phys" / "cuda") if _ROOT else HERE / "_ref" / "no-reference-checkout"
 UNITS = ("outflow.cu", "storage.cu", "adaptive_time.cu", "bifurcation.cu", "reservoir.cu", "levee.cu")
 
 

@@ -17,7 +17,13 @@ import os
 import sys
 import types
 
-REF = os.environ.get("CMF_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", ".."))
+from oracle.refroot import reference_root  # noqa: E402
+
+_root = reference_root()
+if _root is None:
+    raise RuntimeError("the reference checkout is not available (set CMF_REFERENCE_ROOT)")
+REF = str(_root)
 STUBBED = ("hydroforge", "netCDF4", "cftime")
 
 

@@ -2,7 +2,7 @@
 
     python tests/golden/make_topology_golden.py
 
-Runs in the development container only (it reads /root/reference).  On seeded
+Runs only where the reference checkout exists (oracle/refroot.py locates it).  On seeded
 synthetic networks it executes, unmodified:
   cmfgpu/params/utils.py   topological_sort, build_upstream_csr,
                            compute_init_river_depth (numba)
