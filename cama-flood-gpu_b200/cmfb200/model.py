@@ -52,8 +52,15 @@ class Module(SimpleNamespace):
 class InputProxy(dict):
     """Mapping of field name -> array, the role of hydroforge's InputProxy.
 
-    `from_npz` reads an .npz with the reference field names (parameters.nc
-    variables); `from_dict` wraps arrays already in memory."""
+    `from_nc` reads a parameter file with the reference's field names and
+    axes (cmfb200.params: NetCDF classic or .npz; NETCDF4/HDF5 is rejected
+    with the conversion to use), `from_npz` an .npz of the same variables,
+    `from_dict` wraps arrays already in memory."""
+
+    @classmethod
+    def from_nc(cls, path: str) -> "InputProxy":
+        from .params import read_parameters
+        return cls(read_parameters(path))
 
     @classmethod
     def from_dict(cls, fields: Mapping[str, np.ndarray]) -> "InputProxy":
@@ -625,13 +632,50 @@ class CaMaFlood:
     def _stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
 
+    def _order_index(self, inverse: bool) -> torch.Tensor:
+        """Device index tensor of the catchment permutation (cached)."""
+        key = "_inverse_dev" if inverse else "_order_dev"
+        t = getattr(self, key, None)
+        if t is None:
+            t = torch.as_tensor(self.inverse_order if inverse else self.order, device=self.device)
+            setattr(self, key, t)
+        return t
+
     @torch.inference_mode()
-    def set_inputs(self, runoff, inflow=None, sea_surface_elevation=None) -> None:
-        """Stage forcing (cama_flood_model.py:74-102); runoff in model order, m^3/s."""
+    def set_inputs(self, runoff, inflow=None, sea_surface_elevation=None,
+                   order: str = "model") -> None:
+        """Stage forcing (cama_flood_model.py:74-102): runoff in m^3/s, [N] or
+        [N, M].  `order` names the catchment order of `runoff`: "model" (the
+        order of base.catchment_id, which a forcing map built from those ids
+        produces) or "input" (the order of the catchment_id this model was
+        built from -- the reference model's own order, when the fields came
+        from it); "input" runoff is permuted on the device."""
         if inflow is not None or sea_surface_elevation is not None:
             raise ValueError("inflow / sea_level modules are not part of this model")
+        if order not in ("model", "input"):
+            raise ValueError("order must be 'model' or 'input'")
         src = torch.as_tensor(runoff)
+        if order == "input":
+            src = src.to(self.device, non_blocking=True).reshape(self.base.runoff.shape)
+            src = src.index_select(0, self._order_index(False))
         self.base.runoff.copy_(src.reshape(self.base.runoff.shape), non_blocking=True)
+
+    def read_state(self, names: Optional[Iterable[str]] = None,
+                   order: str = "model") -> dict[str, torch.Tensor]:
+        """Copies of state tensors (all of state_tensors() by default).  With
+        order="input" the catchment fields are permuted back to the order of
+        the catchment_id this model was built from; path fields keep their
+        order."""
+        if order not in ("model", "input"):
+            raise ValueError("order must be 'model' or 'input'")
+        st = self.state_tensors()
+        out = {}
+        for k in (list(st) if names is None else list(names)):
+            v = st[k] if k in st else getattr(self.base, k)
+            if order == "input" and not k.startswith("bifurcation_"):
+                v = v.index_select(0, self._order_index(True))
+            out[k] = v.clone()
+        return out
 
     @torch.inference_mode()
     def step_advance(self, num_sub_steps: Optional[int] = None) -> None:
@@ -696,15 +740,26 @@ class CaMaFlood:
         self.compute_stage(diag=True)
 
     def compute_flood_stage_log(self) -> None:
-        """compute_flood_stage; the water budget accumulates when the model
-        was built with the log module."""
+        """compute_flood_stage with the water budget.  The reference's _log
+        kernels add per-sub-step fp32 sums (x 1e-9) into log buffers indexed
+        by the current step; here the fused stage kernel folds the same
+        storage terms, in fp64 and in a fixed order, into per-CTA partials
+        that flush_budget() (and every step_advance) reduces into
+        log.budget.  Like the reference's, it needs the log module (or
+        budget=True): without it there is no budget to write, and it raises."""
+        if not self.budget_enabled:
+            raise ValueError("compute_flood_stage_log needs the log module (or budget=True)")
         self.compute_stage(diag=True)
 
     def compute_levee_stage(self) -> None:
         """Part of compute_flood_stage."""
 
     def compute_levee_stage_log(self) -> None:
-        """Part of compute_flood_stage."""
+        """Part of compute_flood_stage_log (the levee re-partition conserves
+        the cell's storage, so the budget needs no levee term); needs the
+        log module like it."""
+        if not self.budget_enabled:
+            raise ValueError("compute_levee_stage_log needs the log module (or budget=True)")
 
     def launch_substep_kernel(self, k: int, part: int) -> None:
         """Launch one kernel of sub-step k directly (for per-kernel timing)."""
