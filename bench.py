@@ -617,6 +617,7 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96, repeats: int 
             "fwd_adj_over_fwd": t_adj / t_fwd,
             "repeats": reps, "fwd_adj_over_fwd_each": each,
             "fwd_adj_over_fwd_spread": (max(each) - min(each)) / statistics.median(each),
+            "fwd_s_each": tf, "fwd_adj_s_each": ta,
             "product_fwd_value": n * subs / t_prod, "fwd_adj_over_product_fwd": t_adj / t_prod,
             "fwd_adj_over_mixed_product_fwd": t_adj / t_mixed,
             "mixed_product_fwd_ms": t_mixed * 1e3,

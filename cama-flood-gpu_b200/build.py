@@ -21,7 +21,7 @@ INCLUDE = ROOT / "include"
 OUT_DIR = HERE / "cmfb200" / "lib"
 OUT = OUT_DIR / "libcmfb200.so"
 SOURCES = [CSRC / "cmf_plan.cu", CSRC / "cmf_adjoint.cu", CSRC / "cmf_forcing.cu", CSRC / "cmf_topology.cpp"]
-DEPS = SOURCES + [CSRC / "cmf_device.cuh", INCLUDE / "cmfb200.h"]
+DEPS = SOURCES + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "cmfb200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

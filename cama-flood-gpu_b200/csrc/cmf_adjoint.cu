@@ -51,6 +51,7 @@
 // have derivative 0 at 0.
 
 #include "cmfb200.h"
+#include "cmf_physics.cuh"
 
 #include <cstdint>
 #include <cstring>
@@ -91,6 +92,8 @@ __device__ __forceinline__ void pdl_begin()
 
 namespace {
 
+using namespace cmf;
+
 // ---------------------------------------------------------------------------
 // layout
 // ---------------------------------------------------------------------------
@@ -112,69 +115,10 @@ constexpr int kMaxFloodLevels = 16;
 constexpr double kFloor = 1e-6;
 constexpr double kFloor2 = 1e-6 * 1e-6;
 
-// ---------------------------------------------------------------------------
-// forward-mode dual number
-// ---------------------------------------------------------------------------
-struct Dual {
-    double v, d;
-};
-__device__ __forceinline__ Dual D(double v) { return {v, 0.0}; }
-__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-__device__ __forceinline__ Dual operator/(Dual a, Dual b)
-{
-    const double q = a.v / b.v;
-    return {q, (a.d - q * b.d) / b.v};
-}
-__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
-__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
-__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
-__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
-__device__ __forceinline__ Dual operator/(double a, Dual b)
-{
-    const double q = a / b.v;
-    return {q, -q * b.d / b.v};
-}
-
-__device__ __forceinline__ double val(double x) { return x; }
-__device__ __forceinline__ double val(Dual x) { return x.v; }
-__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
-__device__ __forceinline__ double vmin(double a, double b) { return fmin(a, b); }
-__device__ __forceinline__ Dual vmax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
-__device__ __forceinline__ Dual vmin(Dual a, Dual b) { return a.v <= b.v ? a : b; }
-__device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
-__device__ __forceinline__ Dual vsqrt(Dual a)
-{
-    const double s = sqrt(a.v);
-    return {s, a.v > 0.0 ? a.d / (2.0 * s) : 0.0};
-}
-__device__ __forceinline__ double vcbrt(double a) { return cbrt(a); }
-__device__ __forceinline__ Dual vcbrt(Dual a)
-{
-    const double c = cbrt(a.v);
-    return {c, a.v != 0.0 ? a.d / (3.0 * c * c) : 0.0};
-}
-__device__ __forceinline__ double vexp(double a) { return exp(a); }
-__device__ __forceinline__ Dual vexp(Dual a)
-{
-    const double e = exp(a.v);
-    return {e, e * a.d};
-}
-__device__ __forceinline__ double vlog(double a) { return log(a); }
-__device__ __forceinline__ Dual vlog(Dual a) { return {log(a.v), a.d / a.v}; }
-__device__ __forceinline__ double vabs(double a) { return fabs(a); }
-__device__ __forceinline__ Dual vabs(Dual a)
-{
-    return {fabs(a.v), (double)((a.v > 0.0) - (a.v < 0.0)) * a.d};
-}
+// Dual numbers, the scalar operations and the per-element physics are shared
+// with the forward kernels (cmf_scalar.cuh, cmf_physics.cuh).
 template <typename T>
 __device__ __forceinline__ T cnst(double x) { return T(x); }
-template <>
-__device__ __forceinline__ Dual cnst<Dual>(double x) { return D(x); }
 
 // ---------------------------------------------------------------------------
 // context
@@ -232,265 +176,93 @@ __device__ __forceinline__ const double* braw_of(const Ctx& c, const double* X) 
 // templated scalar branches
 // ---------------------------------------------------------------------------
 
-// Reservoir release (reservoir.cu:18-94).
+// Reservoir release of a dam cell (dam_release, reservoir.cu:18-94).
 template <typename T>
 __device__ __forceinline__ T release(const Ctx& c, int slot, T rs, T fs, T total_inflow, T runoff_v,
                                      double time_step)
 {
-    T total = rs + fs;
-    T inflow = total_inflow + runoff_v;
-    const double cons = c.rcons[slot], emerg = c.remerg[slot], adj = c.radj[slot];
-    const double n_out = c.rnout[slot], a_out = c.raout[slot], fc_out = c.rfcout[slot];
-    T ro;
-    if (val(total) <= cons) {
-        ro = n_out * vsqrt(total / cons);
-    } else if (val(total) <= adj) {
-        T frac2 = (total - cons) / (adj - cons);
-        ro = n_out + vexp(3.0 * vlog(frac2)) * (a_out - n_out);
-    } else if (val(total) <= emerg) {
-        T frac3 = (total - adj) / (emerg - adj);
-        T tmp = a_out + vexp(0.1 * vlog(frac3)) * (fc_out - a_out);
-        if (val(inflow) >= fc_out) {
-            T flood = n_out + ((total - cons) / (emerg - cons)) * (inflow - n_out);
-            ro = vmax(flood, tmp);
-        } else {
-            ro = tmp;
-        }
-    } else {
-        ro = (val(inflow) >= fc_out) ? inflow : cnst<T>(fc_out);
-    }
-    ro = vmax(ro, cnst<T>(0.0));
-    ro = vmin(ro, total / time_step);
-    return ro;
+    const DamRule<double> rule{c.rcons[slot], c.radj[slot], c.remerg[slot],
+                               c.rnout[slot], c.raout[slot], c.rfcout[slot]};
+    return dam_release(rule, rs + fs, total_inflow + runoff_v, time_step);
 }
 
-// Kinematic flow of a cell right upstream of a dam (outflow.cu:137-153).
+// Kinematic flow of a cell right upstream of a dam (kinematic_outflow,
+// outflow.cu:137-153); the bed slope depends on the geometry alone.
 template <typename T>
 __device__ __forceinline__ void kinematic(const Ctx& c, long i, T r_dep, T f_dep, T rs, T fs, T r_wid,
                                           T r_man, T f_man, double time_step, T& kin_riv, T& kin_fld)
 {
     const int dn = c.dn[i];
-    double bed_slope = (c.celv[i] - c.celv[dn]) / c.dnd[i];
-    bed_slope = fmax(bed_slope, c.min_kin);
-    T kin_riv_vel = (1.0 / r_man) * sqrt(bed_slope) * vcbrt(r_dep * r_dep);
-    kin_riv = r_wid * r_dep * kin_riv_vel;
-    kin_riv = vmin(kin_riv, rs / time_step);
-    kin_riv = vmax(kin_riv, cnst<T>(0.0));
-    const double bed_slope_f = fmin(bed_slope, 0.005);
-    T kin_fld_vel = (1.0 / f_man) * sqrt(bed_slope_f) * vcbrt(f_dep * f_dep);
-    T kin_fld_area = vmax(fs / c.rl[i] - f_dep * r_wid, cnst<T>(0.0));
-    kin_fld = kin_fld_area * kin_fld_vel;
-    kin_fld = vmin(kin_fld, fs / time_step);
-    kin_fld = vmax(kin_fld, cnst<T>(0.0));
+    const double bed_slope = fmax((c.celv[i] - c.celv[dn]) / c.dnd[i], c.min_kin);
+    kinematic_outflow(bed_slope, c.rl[i], r_dep, f_dep, rs, fs, r_wid, r_man, f_man, time_step,
+                      kin_riv, kin_fld);
 }
 
-// Path momentum with the path limiter (bifurcation.cu:21-129,
-// levee.cu:263-341): in = (wse_c, wse_d, pwse_c, pwse_d, tot_c, tot_d,
-// outflow[L], cross-section depth[L]); out = limited level fluxes, their
-// limited sum and the new cross-section depths.
+// Level fields of path p: the parameters from the plan, the previous flux
+// and depth from the input vector of path_flux.
+template <typename T>
+struct InputPathLevels {
+    const Ctx& c;
+    long p;
+    const T* in;
+    T* depth_out;
+    __device__ double sill(int l) const { return c.belv[p * c.L + l]; }
+    __device__ double width(int l) const { return c.bwid[p * c.L + l]; }
+    __device__ double manning(int l) const { return c.bman[p * c.L + l]; }
+    __device__ T flux(int l) const { return in[6 + l]; }
+    __device__ T depth(int l) const { return in[6 + c.L + l]; }
+    __device__ void new_depth(int l, T h) const { depth_out[l] = h; }
+};
+
+// Path momentum with the path limiter (path_level_fluxes and path_rate,
+// bifurcation.cu:21-129, levee.cu:263-341): in = (wse_c, wse_d, pwse_c,
+// pwse_d, tot_c, tot_d, outflow[L], cross-section depth[L]); out = limited
+// level fluxes, their limited sum and the new cross-section depths.
 template <typename T>
 __device__ __forceinline__ void path_flux(const Ctx& c, long p, const T* in, double time_step,
                                           T* blim, T& bsum, T* bcsd_new)
 {
-    const int L = c.L;
-    const T wse_c = in[0], wse_d = in[1], pwse_c = in[2], pwse_d = in[3];
-    const T ts_c = in[4], ts_d = in[5];
-    const double gravity = c.g;
-    const double blen = c.blen[p];
-    T max_wse = vmax(wse_c, wse_d);
-    T max_pwse = vmax(pwse_c, pwse_d);
-    T slope = (wse_c - wse_d) / blen;
-    slope = vmin(vmax(slope, cnst<T>(-0.005)), cnst<T>(0.005));
-    T upd[kMaxLevels];
-    T sum_out = cnst<T>(0.0);
-    for (int lv = 0; lv < L; ++lv) {
-        const long lp = p * (long)L + lv;
-        const double elv = c.belv[lp];
-        const T o = in[6 + lv];
-        const T csd = in[6 + L + lv];
-        T upd_csd, sifd;
-        if (c.lev) {
-            T current_max_wse = (lv == 0) ? max_wse : max_pwse;
-            upd_csd = vmax(current_max_wse - elv, cnst<T>(0.0));
-            if (lv == 0) {
-                sifd = vsqrt(upd_csd * csd);
-                if (val(sifd) <= 0.0) sifd = upd_csd;
-            } else {
-                sifd = upd_csd;
-            }
-        } else {
-            upd_csd = vmax(max_wse - elv, cnst<T>(0.0));
-            sifd = vmax(vsqrt(upd_csd * csd), vsqrt(upd_csd * 0.01));
-        }
-        T upd_o = cnst<T>(0.0);
-        if (val(sifd) > 1e-5) {
-            const double man = c.bman[lp];
-            const double w = c.bwid[lp];
-            T unit_o = o / w;
-            T num = w * (unit_o + gravity * time_step * sifd * slope);
-            T den = 1.0 + gravity * time_step * (man * man) * vabs(unit_o)
-                    * (1.0 / (sifd * sifd * vcbrt(sifd)));
-            upd_o = num / den;
-        }
-        sum_out = sum_out + upd_o;
-        bcsd_new[lv] = upd_csd;
-        upd[lv] = upd_o;
-    }
-    T lr_p = cnst<T>(1.0);
-    const double denom = fabs(val(sum_out)) * time_step;
-    if (denom > 0.0) lr_p = vmin(0.05 * vmin(ts_c, ts_d) / (vabs(sum_out) * time_step), cnst<T>(1.0));
-    bsum = sum_out * lr_p;
-    for (int lv = 0; lv < L; ++lv) blim[lv] = upd[lv] * lr_p;
+    const PathEnds<T> ends{in[0], in[1], in[2], in[3], in[4], in[5]};
+    const InputPathLevels<T> lv{c, p, in, bcsd_new};
+    T flux[kMaxLevels];
+    const double gdt = c.g * time_step;
+    const T sum = c.lev ? path_level_fluxes<true>(lv, c.L, ends, c.blen[p], gdt, flux)
+                        : path_level_fluxes<false>(lv, c.L, ends, c.blen[p], gdt, flux);
+    const T rate = path_rate(sum, ends.store_a, ends.store_b, time_step);
+    bsum = sum * rate;
+    for (int l = 0; l < c.L; ++l) blim[l] = flux[l] * rate;
 }
 
-// Levee re-partition (levee.cu:29-261) of a levee cell after its flood stage.
-// in = (river storage, flood storage, river depth, flood depth), geometry =
-// (river width, river height); out = (river, flood, protected storage, river,
-// flood, protected depth); the flooded fraction passes through `ffr` (value
-// only).  T is the scalar of everything the state reaches, G that of what
-// depends on the geometry alone (the floodplain scan): a reverse pass along a
-// state direction runs the scan on plain doubles.
-template <typename T>
-__device__ __forceinline__ T up(double x) { return cnst<T>(x); }
-template <typename T>
-__device__ __forceinline__ T up(const Dual& x) { return x; }
-
+// Levee re-partition of a levee cell after its flood stage (levee_partition,
+// levee.cu:29-261).  in = (river storage, flood storage, river depth, flood
+// depth), geometry = (river width, river height); out = (river, flood,
+// protected storage, river, flood, protected depth); the flooded fraction
+// passes through `ffr` (value only).  T is the scalar of everything the
+// state reaches, G that of what depends on the geometry alone (the profile
+// walks): a reverse pass along a state direction runs them on plain doubles.
 template <typename T, typename G>
 __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, G rw, G rh,
                                            double& ffr, T* out)
 {
     const int slot = c.lslot[ci];
-    const int nl = c.K;
-    const double rl = c.rl[ci], ca = c.ca[ci];
-    const double l_crown = c.lcrown[slot], l_frac = c.lfrac[slot], l_base_h = c.lbase[slot];
-    const T riv_sto_curr = in[0], fld_sto_curr = in[1];
-    const T total_sto = riv_sto_curr + fld_sto_curr;
-    const T r_dep_curr = in[2], fld_depth_curr = in[3];
-    G riv_max_sto = rl * rw * rh;
-    if (!(val(total_sto) >= val(riv_max_sto))) {
-        out[0] = riv_sto_curr;
-        out[1] = fld_sto_curr;
-        out[2] = cnst<T>(0.0);
-        out[3] = r_dep_curr;
-        out[4] = fld_depth_curr;
-        out[5] = cnst<T>(0.0);
-        return;
-    }
-    const double dwth_inc = (ca / rl) / (double)nl;
-    const double levee_dist = l_frac * (ca / rl);
-    G s_curr = riv_max_sto;
-    double dhgt_pre = 0.0;
-    G dwth_pre = rw;
-    G levee_base_sto = riv_max_sto;
-    G levee_fill_sto = riv_max_sto;
-    bool found_base = false, found_fill = false;
-    const int ilev = (int)(l_frac * (double)nl);
-    G dsto_fil_B = cnst<G>(0.0), dwth_fil_B = cnst<G>(0.0);
-    double ddph_fil_B = 0.0, gradient_B = 0.0;
-    bool found_B = false;
-    bool scan_needed = true;
-    const double* row = c.tbl + ci * (long)nl;
-    for (int l = 0; l < nl; ++l) {
-        if (!scan_needed) break;
-        const double depth_val = row[l];
-        const double dhgt_seg = fmax(depth_val - dhgt_pre, 1e-6);
-        G dwth_mid = dwth_pre + 0.5 * dwth_inc;
-        G dsto_seg = rl * dwth_mid * dhgt_seg;
-        G s_next = s_curr + dsto_seg;
-        const double gradient = dhgt_seg / dwth_inc;
-
-        const bool cond_base = (l_base_h > dhgt_pre) && (l_base_h <= depth_val);
-        const double ratio_base = (l_base_h - dhgt_pre) / dhgt_seg;
-        G dsto_base_p = rl * (dwth_pre + 0.5 * ratio_base * dwth_inc) * (ratio_base * dhgt_seg);
-        if (cond_base && !found_base) levee_base_sto = s_curr + dsto_base_p;
-        found_base = found_base || cond_base;
-
-        const bool cond_fill = (l_crown > dhgt_pre) && (l_crown <= depth_val);
-        const double ratio_fill = (l_crown - dhgt_pre) / dhgt_seg;
-        G dsto_fill_p = rl * (dwth_pre + 0.5 * ratio_fill * dwth_inc) * (ratio_fill * dhgt_seg);
-        if (cond_fill && !found_fill) levee_fill_sto = s_curr + dsto_fill_p;
-        found_fill = found_fill || cond_fill;
-
-        const double dhgt_dif_loop = l_crown - l_base_h;
-        G s_top_loop = levee_base_sto + (levee_dist + rw) * dhgt_dif_loop * rl;
-        G dsto_add_wedge = (levee_dist + rw) * (l_crown - depth_val) * rl;
-        G threshold = s_next + dsto_add_wedge;
-
-        const bool cond_check = (l >= ilev) && !found_B;
-        const bool cond_found = cond_check && (val(total_sto) < val(threshold));
-        G current_lb = (l == ilev) ? s_top_loop : dsto_fil_B;
-        if (cond_check && !cond_found) {
-            dsto_fil_B = threshold;
-            dwth_fil_B = cnst<G>(dwth_inc * (double)(l + 1) - levee_dist);
-            ddph_fil_B = depth_val - l_base_h;
-        } else {
-            dsto_fil_B = current_lb;
-        }
-        if (cond_found) gradient_B = gradient;
-        found_B = found_B || cond_found;
-
-        s_curr = s_next;
-        dhgt_pre = depth_val;
-        dwth_pre = dwth_pre + dwth_inc;
-        scan_needed = !(found_base && found_fill && found_B);
-    }
-    G s_base_extra = s_curr + rl * dwth_pre * (l_base_h - dhgt_pre);
-    if (!found_base) levee_base_sto = (l_base_h > dhgt_pre) ? s_base_extra : riv_max_sto;
-    G s_fill_extra = s_curr + rl * dwth_pre * (l_crown - dhgt_pre);
-    if (!found_fill) levee_fill_sto = (l_crown > dhgt_pre) ? s_fill_extra : riv_max_sto;
-
-    const double dhgt_dif = l_crown - l_base_h;
-    G s_top = levee_base_sto + (levee_dist + rw) * dhgt_dif * rl;
-    const bool is_case4 = val(total_sto) >= val(levee_fill_sto);
-    const bool is_case3 = (!is_case4) && (val(total_sto) >= val(s_top));
-    const bool is_case2 = (!is_case4) && (!is_case3) && (val(total_sto) >= val(levee_base_sto));
-
-    T dsto_add_c2 = total_sto - levee_base_sto;
-    G dwth_add_c2 = levee_dist + rw;
-    T f_dph_c2 = l_base_h + dsto_add_c2 / dwth_add_c2 / rl;
-    T r_sto_c2 = riv_max_sto + rl * rw * f_dph_c2;
-    T r_dph_c2 = r_sto_c2 / rl / rw;
-    T f_sto_c2 = vmax(total_sto - r_sto_c2, cnst<T>(0.0));
-    const double f_frc_c2 = l_frac;
-
-    T dsto_add_B = total_sto - dsto_fil_B;
-    T term_B = dwth_fil_B * dwth_fil_B + 2.0 * dsto_add_B / rl / (gradient_B + 1e-9);
-    T dwth_add_B = -dwth_fil_B + vsqrt(vmax(term_B, cnst<T>(0.0)));
-    T ddph_add_B = dwth_add_B * gradient_B;
-    T p_dph_B_found = l_base_h + ddph_fil_B + ddph_add_B;
-    const double f_frc_B_found = (val(dwth_fil_B) + levee_dist) / (dwth_inc * (double)nl);
-    T ddph_add_B_extra = dsto_add_B / (dwth_fil_B * rl + 1e-9);
-    T p_dph_B_extra = l_base_h + ddph_fil_B + ddph_add_B_extra;
-    T p_dph_B = found_B ? p_dph_B_found : p_dph_B_extra;
-    const double f_frc_B = found_B ? f_frc_B_found : 1.0;
-
-    G r_sto_c3 = riv_max_sto + rl * rw * l_crown;
-    G r_dph_c3 = r_sto_c3 / rl / rw;
-    G f_sto_c3 = vmax(s_top - r_sto_c3, cnst<G>(0.0));
-    const double f_frc_c3 = fmin(fmax(f_frc_B, 0.0), 1.0);
-
-    T f_dph_c4 = fld_depth_curr;
-    T dsto_add_c4 = (f_dph_c4 - l_crown) * (levee_dist + rw) * rl;
-    T f_sto_c4 = vmax(s_top + dsto_add_c4 - riv_sto_curr, cnst<T>(0.0));
-
-    T r_sto_candidate = is_case2 ? r_sto_c2 : (is_case3 ? up<T>(r_sto_c3) : riv_sto_curr);
-    T f_sto_candidate = is_case2 ? f_sto_c2 : (is_case3 ? up<T>(f_sto_c3) : (is_case4 ? f_sto_c4 : fld_sto_curr));
-    const bool no_levee_partition = !is_case2 && !is_case3 && !is_case4;
-    T r_sto = (is_case4 || no_levee_partition) ? riv_sto_curr : vmin(r_sto_candidate, total_sto);
-    T remaining_sto = total_sto - r_sto;
-    remaining_sto = val(remaining_sto) > 0.0 ? remaining_sto : cnst<T>(0.0);
-    T f_sto = vmin(val(f_sto_candidate) > 0.0 ? f_sto_candidate : cnst<T>(0.0), remaining_sto);
-    if (is_case2) f_sto = remaining_sto;
-    if (no_levee_partition) f_sto = fld_sto_curr;
-    T p_sto = remaining_sto - f_sto;
-    p_sto = val(p_sto) > 0.0 ? p_sto : cnst<T>(0.0);
-    out[0] = r_sto;
-    out[1] = f_sto;
-    out[2] = p_sto;
-    out[3] = is_case2 ? r_dph_c2 : (is_case3 ? up<T>(r_dph_c3) : r_dep_curr);
-    out[4] = is_case2 ? f_dph_c2 : (is_case3 ? cnst<T>(l_crown) : fld_depth_curr);
-    out[5] = is_case2 ? cnst<T>(0.0) : (is_case3 ? p_dph_B : (is_case4 ? f_dph_c4 : cnst<T>(0.0)));
-    ffr = is_case2 ? f_frc_c2 : (is_case3 ? f_frc_c3 : ffr);
+    LeveeState<T, T> st;
+    st.rs = in[0];
+    st.fs = in[1];
+    st.ps = T(0);
+    st.rdep = in[2];
+    st.fdep = in[3];
+    st.pdep = T(0);
+    st.ffr = T(ffr);
+    const double* row = c.tbl + ci * (long)c.K;
+    levee_partition(st, rw, rh, c.rl[ci], c.ca[ci], c.lcrown[slot], c.lfrac[slot], c.lbase[slot],
+                    c.K, [row](int l) { return row[l]; });
+    out[0] = st.rs;
+    out[1] = st.fs;
+    out[2] = st.ps;
+    out[3] = st.rdep;
+    out[4] = st.fdep;
+    out[5] = st.pdep;
+    ffr = val(st.ffr);
 }
 
 // Contract the Jacobian of a templated branch with output adjoints:
@@ -521,8 +293,8 @@ struct Mom {
     bool mouth, rc, fc, zero_f, neg;
     int dn;
     double rw, rman, fman, rl, rout, fout, fdep, rcsd, fcsd, fcsa;
-    double wse, wse_dn, slope, ucsd, P1, s1, fsurf_m, ufcsd, P2, s2, ufcsa_raw, ufcsa;
-    double r_sifd, f_sifd, q, num, den, qr0_val, fc6, P3, s3, fimp, numf, denf, qf0_val;
+    double wse, wse_dn, slope, hr_now, P1, s1, hf_raw, hf_now, P2, s2, af_raw, af_now;
+    double hr_si, hf_si, q, num, den, qr0_val, fc6, P3, s3, af_si, numf, denf, qf0_val;
     double qr0, qf0, qf1, tnf, lrn_raw, lrn, qr, qf;
 };
 
@@ -547,46 +319,44 @@ __device__ __forceinline__ void mom_eval(const Ctx& c, const double* X, long i, 
     m.fcsa = X[F_FCSA * N + i];
     const double fs = X[F_FS * N + i];
 
-    const double river_elevation = c_elv - r_hgt;
-    m.wse = r_dep + river_elevation;
-    const double r_dep_dn = X[F_RDEP * N + m.dn];
-    const double river_elevation_dn = c.celv[m.dn] - c.rh[m.dn];
-    m.wse_dn = m.mouth ? c_elv : r_dep_dn + river_elevation_dn;
-    const double max_wse = fmax(m.wse, m.wse_dn);
+    // surfaces and interface state as momentum_cell forms them
+    const double bed = c_elv - r_hgt;
+    m.wse = r_dep + bed;
+    m.wse_dn = m.mouth ? c_elv : X[F_RDEP * N + m.dn] + (c.celv[m.dn] - c.rh[m.dn]);
+    const double top = fmax(m.wse, m.wse_dn);
     m.slope = (m.wse - m.wse_dn) / dn_dist;
-    const double fslope = fmin(fmax(m.slope, -0.005), 0.005);
+    const double fslope = capped_slope(m.slope, 0.005);
 
-    m.ucsd = m.mouth ? r_dep : max_wse - river_elevation;
-    m.P1 = m.ucsd * m.rcsd;
+    m.hr_now = m.mouth ? r_dep : top - bed;
+    m.P1 = m.hr_now * m.rcsd;
     m.s1 = sqrt(m.P1);
-    m.r_sifd = fmax(m.s1, kFloor);
-    const double flood_surface = m.mouth ? m.wse : max_wse;
-    m.fsurf_m = flood_surface - c_elv;
-    m.ufcsd = fmax(m.fsurf_m, 0.0);
-    m.P2 = m.ufcsd * m.fcsd;
+    m.hr_si = fmax(m.s1, kFloor);
+    m.hf_raw = (m.mouth ? m.wse : top) - c_elv;
+    m.hf_now = fmax(m.hf_raw, 0.0);
+    m.P2 = m.hf_now * m.fcsd;
     m.s2 = sqrt(m.P2);
-    m.f_sifd = fmax(m.s2, kFloor);
-    m.ufcsa_raw = fs / m.rl - m.fdep * m.rw;
-    m.ufcsa = fmax(m.ufcsa_raw, 0.0);
+    m.hf_si = fmax(m.s2, kFloor);
+    m.af_raw = fs / m.rl - m.fdep * m.rw;
+    m.af_now = fmax(m.af_raw, 0.0);
 
-    const double r_cs_area = m.ucsd * m.rw;
-    m.rc = (m.r_sifd > 1e-5) && (r_cs_area > 1e-5);
+    // river channel: channel_discharge with its terms kept for the reverse
+    m.rc = (m.hr_si > 1e-5) && (m.hr_now * m.rw > 1e-5);
     m.q = m.rout / m.rw;
-    m.num = m.rw * (m.q + c.g * dt * m.r_sifd * m.slope);
+    m.num = m.rw * (m.q + c.g * dt * m.hr_si * m.slope);
     m.den = 1.0 + c.g * dt * (m.rman * m.rman) * fabs(m.q)
-            * (1.0 / (m.r_sifd * m.r_sifd * cbrt(m.r_sifd)));
+            * (1.0 / (m.hr_si * m.hr_si * cbrt(m.hr_si)));
     m.qr0_val = m.num / m.den;
     m.qr0 = m.rc ? m.qr0_val : 0.0;
 
-    m.fc = (m.f_sifd > 1e-5) && (m.ufcsa > 1e-5);
+    m.fc = (m.hf_si > 1e-5) && (m.af_now > 1e-5);
     m.qf0 = 0.0;
     m.fc6 = fmax(m.fcsa, kFloor);
-    m.P3 = m.ufcsa * m.fc6;
+    m.P3 = m.af_now * m.fc6;
     m.s3 = sqrt(m.P3);
-    m.fimp = fmax(m.s3, kFloor);
-    m.numf = m.fout + c.g * dt * m.fimp * fslope;
+    m.af_si = fmax(m.s3, kFloor);
+    m.numf = m.fout + c.g * dt * m.af_si * fslope;
     m.denf = 1.0 + c.g * dt * (m.fman * m.fman) * fabs(m.fout)
-             * (1.0 / (m.f_sifd * cbrt(m.f_sifd))) / m.fimp;
+             * (1.0 / (m.hf_si * cbrt(m.hf_si))) / m.af_si;
     m.qf0_val = m.numf / m.denf;
     if (m.fc) m.qf0 = m.qf0_val;
 
@@ -601,9 +371,9 @@ __device__ __forceinline__ void mom_eval(const Ctx& c, const double* X, long i, 
     if (m.neg) {
         const double rs = X[F_RS * N + i];
         const double ps = X[F_PS * N + i];
-        const double total_storage_f = rs + fs + ps;
+        const double held = rs + fs + ps;
         m.tnf = (-m.qr0 - m.qf1) * dt;
-        m.lrn_raw = 0.05 * total_storage_f / m.tnf;
+        m.lrn_raw = 0.05 * held / m.tnf;
         m.lrn = fmin(m.lrn_raw, 1.0);
         m.qr = m.qr0 * m.lrn;
         m.qf = m.qf1 * m.lrn;
@@ -673,58 +443,38 @@ struct Stage {
 __device__ __forceinline__ void stage_eval(const Ctx& c, long i, double total_s, double rh,
                                            double rw, double rl, Stage& s)
 {
-    const double total_storage = total_s;
     s.rmax = rl * rw * rh;
-    s.flooded = !(total_storage <= s.rmax);
+    s.flooded = !(total_s <= s.rmax);
     s.top = false;
     s.cap_taken = false;
     s.level = 0;
     if (!s.flooded) {
         s.rs = total_s;
         s.fs = 0.0;
-        s.rdep = total_storage / (rl * rw);
+        s.rdep = total_s / (rl * rw);
         s.fdep = 0.0;
         s.ffr = 0.0;
         return;
     }
-    const int nl = c.K;
+    const int K = c.K;
     const double ca = c.ca[i];
-    const double catchment_width = ca / rl;
-    s.winc = catchment_width / (double)nl;
-    double S_accum = s.rmax, prev_H = 0.0, prev_W = rw;
-    double prev_total_storage = s.rmax, prev_flood_depth = 0.0, next_flood_depth = 0.0;
-    const double* row = c.tbl + i * (long)nl;
-    for (int l = 0; l < nl; ++l) {
-        const double H_curr = __ldg(row + l);
-        const double W_curr = rw + (double)(l + 1) * s.winc;
-        const double dS = rl * 0.5 * (prev_W + W_curr) * (H_curr - prev_H);
-        const double S_curr = S_accum + dS;
-        next_flood_depth = H_curr;
-        if (total_storage > S_curr) {
-            s.level += 1;
-            prev_total_storage = S_curr;
-            prev_flood_depth = H_curr;
-            S_accum = S_curr;
-            prev_H = H_curr;
-            prev_W = W_curr;
-        } else {
-            break;
-        }
-    }
-    s.top = s.level == nl;
-    s.S_prev = prev_total_storage;
-    s.D_prev = prev_flood_depth;
-    s.W_tot = rw + (double)s.level * s.winc;
-    s.excess = total_storage - prev_total_storage;
-    s.diff_w = 0.0;
-    if (s.top) {
-        s.fdep = prev_flood_depth + s.excess / (s.W_tot * rl);
-    } else {
-        s.grad = (next_flood_depth - prev_flood_depth) / s.winc;
+    s.winc = ca / rl / (double)K;
+    // where the storage lies on the floodplain profile (fill_level_mem,
+    // flood_surface), with the quantities the reverse needs kept
+    const FillLevel<double> f = fill_level_mem(c.tbl + i * (long)K, K, total_s, s.rmax, rw, rl, s.winc);
+    const FloodSurface<double> surf = flood_surface(f, K, total_s, rw, rl, s.winc);
+    s.level = f.full;
+    s.top = f.full == K;
+    s.S_prev = f.s_top;
+    s.D_prev = f.d_top;
+    s.W_tot = surf.width_top;
+    s.excess = total_s - f.s_top;
+    s.diff_w = surf.extra_width;
+    s.fdep = surf.depth;
+    if (!s.top) {
+        s.grad = (f.d_next - f.d_top) / s.winc;
         s.arg = s.W_tot * s.W_tot + 2.0 * s.excess / (s.grad * rl);
         s.sq = sqrt(s.arg);
-        s.diff_w = s.sq - s.W_tot;
-        s.fdep = prev_flood_depth + s.diff_w * s.grad;
     }
     s.cap = s.rmax + rl * rw * s.fdep;
     s.cap_taken = s.cap < total_s;
@@ -733,10 +483,9 @@ __device__ __forceinline__ void stage_eval(const Ctx& c, long i, double total_s,
     double ff = (s.W_tot + s.diff_w - rw) * rl / ca;
     ff = ff < 0.0 ? 0.0 : (ff > 1.0 ? 1.0 : ff);
     s.ffr = s.top ? 1.0 : ff;
-    double flood = total_s - river;
-    if (flood < 0.0) flood = 0.0;
+    const double flood = total_s - river;
     s.rs = river;
-    s.fs = flood;
+    s.fs = flood < 0.0 ? 0.0 : flood;
 }
 
 // Reverse of stage_eval: output adjoints (river/flood storage, river/flood
@@ -883,9 +632,9 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) ka_momentum(const 
     const long N = c.N;
     X[F_QR * N + i] = qr;
     X[F_QF * N + i] = qf;
-    Y[F_RCSD * N + i] = m.ucsd;
-    Y[F_FCSD * N + i] = m.ufcsd;
-    Y[F_FCSA * N + i] = m.ufcsa;
+    Y[F_RCSD * N + i] = m.hr_now;
+    Y[F_FCSD * N + i] = m.hf_now;
+    Y[F_FCSA * N + i] = m.af_now;
 }
 
 __device__ __forceinline__ double outgoing(const Ctx& c, const double* X, long i, double dt)
@@ -1454,9 +1203,9 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const 
         if (qr_final <= 0.0) qr_bar += -ogb_dn * dt;
         if (qf_final <= 0.0) qf_bar += -ogb_dn * dt;
     }
-    double ucsd_bar = lam[F_RCSD * N + i];
-    double ufcsd_bar = lam[F_FCSD * N + i];
-    double ufcsa_bar = lam[F_FCSA * N + i];
+    double hr_now_bar = lam[F_RCSD * N + i];
+    double hf_now_bar = lam[F_FCSD * N + i];
+    double af_now_bar = lam[F_FCSA * N + i];
 
     double rs_bar = 0.0, fs_bar = 0.0, ps_bar = 0.0, rout_bar = 0.0, fout_bar = 0.0, rdep_bar = 0.0;
     double fdep_bar = 0.0, rcsd_bar = 0.0, fcsd_bar = 0.0, fcsa_bar = 0.0;
@@ -1487,68 +1236,68 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const 
     }
     const double qf0_bar = m.zero_f ? 0.0 : qf1_bar;
 
-    double slope_bar = 0.0, fslope_bar = 0.0, r_sifd_bar = 0.0, f_sifd_bar = 0.0;
+    double slope_bar = 0.0, fslope_bar = 0.0, hr_si_bar = 0.0, hf_si_bar = 0.0;
     if (m.fc) {
         const double numf_bar = qf0_bar / m.denf;
         const double denf_bar = -qf0_bar * m.qf0_val / m.denf;
         fout_bar += numf_bar;
-        double fimp_bar = numf_bar * Dg * fmin(fmax(m.slope, -0.005), 0.005);
-        fslope_bar += numf_bar * Dg * m.fimp;
+        double af_si_bar = numf_bar * Dg * fmin(fmax(m.slope, -0.005), 0.005);
+        fslope_bar += numf_bar * Dg * m.af_si;
         const double af = fabs(m.fout);
-        const double B = 1.0 / (m.f_sifd * cbrt(m.f_sifd));
+        const double B = 1.0 / (m.hf_si * cbrt(m.hf_si));
         const double nf2 = m.fman * m.fman;
-        const double T = Dg * nf2 * af * B / m.fimp;
-        g_fman += denf_bar * Dg * 2.0 * m.fman * af * B / m.fimp;
-        fout_bar += denf_bar * Dg * nf2 * B / m.fimp * sgn(m.fout);
-        f_sifd_bar += denf_bar * Dg * nf2 * af / m.fimp * (-(4.0 / 3.0) * B / m.f_sifd);
-        fimp_bar += denf_bar * (-T / m.fimp);
+        const double T = Dg * nf2 * af * B / m.af_si;
+        g_fman += denf_bar * Dg * 2.0 * m.fman * af * B / m.af_si;
+        fout_bar += denf_bar * Dg * nf2 * B / m.af_si * sgn(m.fout);
+        hf_si_bar += denf_bar * Dg * nf2 * af / m.af_si * (-(4.0 / 3.0) * B / m.hf_si);
+        af_si_bar += denf_bar * (-T / m.af_si);
         if (m.P3 > kFloor2) {
-            const double P3_bar = fimp_bar / (2.0 * m.s3);
-            ufcsa_bar += P3_bar * m.fc6;
-            if (m.fcsa >= kFloor) fcsa_bar += P3_bar * m.ufcsa;
+            const double P3_bar = af_si_bar / (2.0 * m.s3);
+            af_now_bar += P3_bar * m.fc6;
+            if (m.fcsa >= kFloor) fcsa_bar += P3_bar * m.af_now;
         }
     }
     if (m.rc) {
         const double num_bar = qr0_bar / m.den;
         const double den_bar = -qr0_bar * m.qr0_val / m.den;
-        g_rw += num_bar * (m.q + Dg * m.r_sifd * m.slope);
+        g_rw += num_bar * (m.q + Dg * m.hr_si * m.slope);
         const double inner_bar = num_bar * m.rw;
         double q_bar = inner_bar;
-        r_sifd_bar += inner_bar * Dg * m.slope;
-        slope_bar += inner_bar * Dg * m.r_sifd;
+        hr_si_bar += inner_bar * Dg * m.slope;
+        slope_bar += inner_bar * Dg * m.hr_si;
         const double aq = fabs(m.q);
-        const double Br = 1.0 / (m.r_sifd * m.r_sifd * cbrt(m.r_sifd));
+        const double Br = 1.0 / (m.hr_si * m.hr_si * cbrt(m.hr_si));
         const double n2 = m.rman * m.rman;
         g_rman += den_bar * Dg * 2.0 * m.rman * aq * Br;
         q_bar += den_bar * Dg * n2 * Br * sgn(m.q);
-        r_sifd_bar += den_bar * Dg * n2 * aq * (-(7.0 / 3.0) * Br / m.r_sifd);
+        hr_si_bar += den_bar * Dg * n2 * aq * (-(7.0 / 3.0) * Br / m.hr_si);
         rout_bar += q_bar / m.rw;
         g_rw += -q_bar * m.q / m.rw;
     }
     if (m.slope >= -0.005 && m.slope <= 0.005) slope_bar += fslope_bar;
-    if (m.ufcsa_raw >= 0.0) {
-        fs_bar += ufcsa_bar / m.rl;
-        fdep_bar += -ufcsa_bar * m.rw;
-        g_rw += -ufcsa_bar * m.fdep;
+    if (m.af_raw >= 0.0) {
+        fs_bar += af_now_bar / m.rl;
+        fdep_bar += -af_now_bar * m.rw;
+        g_rw += -af_now_bar * m.fdep;
     }
     if (m.P2 > kFloor2) {
-        const double P2_bar = f_sifd_bar / (2.0 * m.s2);
-        ufcsd_bar += P2_bar * m.fcsd;
-        fcsd_bar += P2_bar * m.ufcsd;
+        const double P2_bar = hf_si_bar / (2.0 * m.s2);
+        hf_now_bar += P2_bar * m.fcsd;
+        fcsd_bar += P2_bar * m.hf_now;
     }
-    double fsurf_bar = (m.fsurf_m >= 0.0) ? ufcsd_bar : 0.0;
+    double fsurf_bar = (m.hf_raw >= 0.0) ? hf_now_bar : 0.0;
     if (m.P1 > kFloor2) {
-        const double P1_bar = r_sifd_bar / (2.0 * m.s1);
-        ucsd_bar += P1_bar * m.rcsd;
-        rcsd_bar += P1_bar * m.ucsd;
+        const double P1_bar = hr_si_bar / (2.0 * m.s1);
+        hr_now_bar += P1_bar * m.rcsd;
+        rcsd_bar += P1_bar * m.hr_now;
     }
     double wse_bar = 0.0, wse_dn_bar = 0.0, mw_bar = 0.0;
     if (m.mouth) {
-        rdep_bar += ucsd_bar;
+        rdep_bar += hr_now_bar;
         wse_bar += fsurf_bar;
     } else {
-        mw_bar += ucsd_bar;
-        relev_bar -= ucsd_bar;
+        mw_bar += hr_now_bar;
+        relev_bar -= hr_now_bar;
         mw_bar += fsurf_bar;
     }
     wse_bar += slope_bar / c.dnd[i];

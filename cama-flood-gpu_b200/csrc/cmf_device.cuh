@@ -27,18 +27,19 @@
 // order (the member tile, see tile_elem); W = 1 for one member.
 //
 // Catchments are stored breadth-first from the mouths, so the upstream cells
-// of p are [up[p], up[p+1]) and no upstream index array exists.  Every float
-// expression keeps the operand order of the reference kernels it replaces so
-// that float rounding matches (cmfgpu/phys/cuda: outflow.cu, reservoir.cu,
-// bifurcation.cu, storage.cu, levee.cu, adaptive_time.cu).  Storage is fp64
-// ("STO") and ping-pongs between two buffers inside an interval so the
-// limiter can read pre-update storage of neighbours while cells update their
-// own.
+// of p are [up[p], up[p+1]) and no upstream index array exists.  This file
+// holds the kernels' data movement (layout, gathers, member tiles, step
+// control); the per-element physics is cmf_physics.cuh, whose rounded
+// operation sequences are those of the reference kernels (cmfgpu/phys/cuda),
+// so results match them bit for bit.  Storage is fp64 ("STO") and
+// ping-pongs between two buffers inside an interval so the limiter can read
+// pre-update storage of neighbours while cells update their own.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "cmfb200.h"
+#include "cmf_physics.cuh"
 
 // minimum resident 256-thread CTAs per SM (register caps) of the sub-step kernels;
 // k_stage: 4 (64 registers, no spills)
@@ -174,8 +175,6 @@ __device__ __forceinline__ REAL par(const REAL* p, int bit, int batched, long i,
     return p[(ONE || !(batched & bit)) ? i : i * (long)M + m];
 }
 
-template <typename REAL>
-__device__ __forceinline__ REAL pow73(REAL x) { return x * x * cbrt(x); }
 
 // End of the upstream range of cell x.  In the basin-major breadth-first
 // order a basin's mouth sits right before its own upstream cells, so when
@@ -235,7 +234,10 @@ __device__ __forceinline__ StepInfo step_info(const int* ctl, const int* nsub, i
 }
 
 // ---------------------------------------------------------------------------
-// k_momentum: cell part (outflow.cu:21-175, reservoir.cu:18-94)
+// k_momentum, cell part: a catchment's outflow over the sub-step
+// (outflow.cu:21-175, reservoir.cu:18-94), from the physics of
+// cmf_physics.cuh.  Writes the unlimited river and floodplain fluxes and the
+// new interface state (flow depths, floodplain flow area).
 // ---------------------------------------------------------------------------
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF>
 __device__ __forceinline__ void momentum_cell(const Dev<REAL>& v, long i, int m, int kh,
@@ -243,286 +245,185 @@ __device__ __forceinline__ void momentum_cell(const Dev<REAL>& v, long i, int m,
 {
     const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
     if (!st.active) return;
-    const bool diag = st.diag;
-    const int k = st.k;
-    const double* __restrict__ rsrc = (k & 1) ? v.rs1 : v.rs0;
-    const double* __restrict__ fsrc = (k & 1) ? v.fs1 : v.fs0;
+    const double* __restrict__ rsrc = (st.k & 1) ? v.rs1 : v.rs0;
+    const double* __restrict__ fsrc = (st.k & 1) ? v.fs1 : v.fs0;
     const int M = v.M;
     const long im = ix<ONE>(i, m, M);
-    const REAL time_step = v.dt[m];
-    const REAL gravity = v.g;
+    const REAL dt = v.dt[m];
+    const REAL gdt = v.g * dt;
     const uint8_t fl = v.flags[i];
     const bool mouth = fl & CMF_CELL_MOUTH;
-    const int dn = v.dn[i];
-
-    REAL r_out = v.rout[im];
-    REAL r_man = par<ONE>(v.rman, CMF_BATCH_RIVER_MANNING, v.batched, i, m, M);
-    REAL r_dep = v.rdep[im];
-    REAL r_wid = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, i, m, M);
-    REAL r_len = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, i, m, M);
-    REAL r_hgt = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, i, m, M);
-    REAL f_out = v.fout[im];
-    REAL f_man = par<ONE>(v.fman, CMF_BATCH_FLOOD_MANNING, v.batched, i, m, M);
-    REAL f_dep = v.fdep[im];
-    REAL c_elv = v.celv[i];
-    REAL dn_dist = v.dnd[i];
-    REAL r_cs_dep = v.rcsd[im];
-    REAL f_cs_dep = v.fcsd[im];
-    REAL f_cs_area = v.fcsa[im];
-    REAL fs = (REAL)fsrc[im];
-
-    REAL river_elevation = c_elv - r_hgt;
-    REAL wse = r_dep + river_elevation;
-
-    const long dm = ix<ONE>(dn, m, M);
-    REAL r_dep_dn = v.rdep[dm];
-    REAL r_hgt_dn = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, dn, m, M);
-    REAL c_elv_dn = v.celv[dn];
-    REAL river_elevation_dn = c_elv_dn - r_hgt_dn;
-    REAL wse_dn = r_dep_dn + river_elevation_dn;
-    if (mouth) wse_dn = c_elv;
-    REAL max_wse = fmax(wse, wse_dn);
-
-    REAL river_slope = (wse - wse_dn) / dn_dist;
-    REAL flood_slope = fmin(fmax(river_slope, (REAL)-0.005), (REAL)0.005);
-
-    REAL upd_r_cs_dep = mouth ? r_dep : max_wse - river_elevation;
-    REAL r_sifd = fmax(sqrt(upd_r_cs_dep * r_cs_dep), (REAL)1e-6);
-    REAL flood_surface = mouth ? wse : max_wse;
-    REAL upd_f_cs_dep = fmax(flood_surface - c_elv, (REAL)0.0);
-    REAL f_sifd = fmax(sqrt(upd_f_cs_dep * f_cs_dep), (REAL)1e-6);
-    REAL upd_f_cs_area = fmax(fs / r_len - f_dep * r_wid, (REAL)0.0);
-
-    REAL r_cs_area = upd_r_cs_dep * r_wid;
-    bool river_condition = (r_sifd > (REAL)1e-5) && (r_cs_area > (REAL)1e-5);
-    REAL unit_r_out = r_out / r_wid;
-    REAL num_r = r_wid * (unit_r_out + gravity * time_step * r_sifd * river_slope);
-    REAL den_r = (REAL)1.0 + gravity * time_step * (r_man * r_man) * fabs(unit_r_out)
-                 * ((REAL)1.0 / (r_sifd * r_sifd * cbrt(r_sifd)));
-    REAL upd_r_out = num_r / den_r;
-    upd_r_out = river_condition ? upd_r_out : (REAL)0.0;
-
-    bool flood_condition = (f_sifd > (REAL)1e-5) && (upd_f_cs_area > (REAL)1e-5);
-    REAL upd_f_out = (REAL)0.0;
-    if (flood_condition) {
-        REAL f_imp_area = fmax(sqrt(upd_f_cs_area * fmax(f_cs_area, (REAL)1e-6)), (REAL)1e-6);
-        REAL num_f = f_out + gravity * time_step * f_imp_area * flood_slope;
-        REAL den_f = (REAL)1.0 + gravity * time_step * (f_man * f_man) * fabs(f_out)
-                     * ((REAL)1.0 / (f_sifd * cbrt(f_sifd))) / f_imp_area;
-        upd_f_out = num_f / den_f;
-    }
-
-    if ((upd_r_out * upd_f_out) < (REAL)0.0) upd_f_out = (REAL)0.0;
     const bool lev_cell = LEV && (fl & CMF_CELL_LEVEE);
-    bool is_negative_flow = (upd_r_out < (REAL)0.0) && !mouth;
-    REAL rs = (REAL)0;
-    bool rs_loaded = false;
-    if (is_negative_flow) {
-        rs = (REAL)rsrc[im];
-        rs_loaded = true;
-        REAL ps = lev_cell ? (REAL)v.ps[im] : (REAL)0;
-        REAL total_storage_f = rs + fs + ps;
-        REAL total_negative_flow = (-upd_r_out - upd_f_out) * time_step;
-        REAL limit_rate = fmin((REAL)0.05 * total_storage_f / total_negative_flow, (REAL)1.0);
-        upd_r_out *= limit_rate;
-        upd_f_out *= limit_rate;
-    }
-
-    if (RES && (fl & CMF_CELL_DAM_UPSTREAM)) {
-        if (!rs_loaded) { rs = (REAL)rsrc[im]; rs_loaded = true; }
-        REAL bed_slope = (c_elv - c_elv_dn) / dn_dist;
-        bed_slope = fmax(bed_slope, v.min_kin);
-        REAL kin_riv_vel = ((REAL)1.0 / r_man) * sqrt(bed_slope) * cbrt(r_dep * r_dep);
-        REAL kin_riv = r_wid * r_dep * kin_riv_vel;
-        kin_riv = fmin(kin_riv, rs / time_step);
-        kin_riv = fmax(kin_riv, (REAL)0.0);
-        REAL bed_slope_f = fmin(bed_slope, (REAL)0.005);
-        REAL kin_fld_vel = ((REAL)1.0 / f_man) * sqrt(bed_slope_f) * cbrt(f_dep * f_dep);
-        REAL kin_fld_area = fmax(fs / r_len - f_dep * r_wid, (REAL)0.0);
-        REAL kin_fld = kin_fld_area * kin_fld_vel;
-        kin_fld = fmin(kin_fld, fs / time_step);
-        kin_fld = fmax(kin_fld, (REAL)0.0);
-        upd_r_out = kin_riv;
-        upd_f_out = kin_fld;
-    }
-
-    REAL res_total = (REAL)0;
     const bool res_cell = RES && (fl & CMF_CELL_RESERVOIR);
-    if (res_cell) {
-        // reservoir.cu:18-94: the release replaces the local-inertial flux;
-        // undo/redo of the outgoing scatter is implicit because the limiter
-        // gathers qu directly.
-        if (!rs_loaded) { rs = (REAL)rsrc[im]; rs_loaded = true; }
-        const int slot = v.rslot[i];
-        REAL total = rs + fs;
-        res_total = total;
-        REAL total_inflow = (REAL)v.rti[im];
-        REAL runoff_v = par<ONE>(v.runoff, CMF_BATCH_RUNOFF, v.batched, i, m, M);
-        REAL inflow = total_inflow + runoff_v;
-        REAL cons = v.rcons[slot];
-        REAL emerg = v.remerg[slot];
-        REAL adj = v.radj[slot];
-        REAL n_out = v.rnout[slot];
-        REAL a_out = v.raout[slot];
-        REAL fc_out = v.rfcout[slot];
-        REAL ro;
-        if (total <= cons) {
-            ro = n_out * sqrt(total / cons);
-        } else if (total <= adj) {
-            REAL frac2 = (total - cons) / (adj - cons);
-            ro = n_out + exp((REAL)3.0 * log(frac2)) * (a_out - n_out);
-        } else if (total <= emerg) {
-            REAL frac3 = (total - adj) / (emerg - adj);
-            REAL tmp = a_out + exp((REAL)0.1 * log(frac3)) * (fc_out - a_out);
-            if (inflow >= fc_out) {
-                REAL flood = n_out + ((total - cons) / (emerg - cons)) * (inflow - n_out);
-                ro = fmax(flood, tmp);
-            } else {
-                ro = tmp;
-            }
-        } else {
-            ro = (inflow >= fc_out) ? inflow : fc_out;
+    const int dn = v.dn[i];
+    const long dm = ix<ONE>(dn, m, M);
+
+    const REAL width = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, i, m, M);
+    const REAL len = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, i, m, M);
+    const REAL bank_h = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, i, m, M);
+    const REAL n_riv = par<ONE>(v.rman, CMF_BATCH_RIVER_MANNING, v.batched, i, m, M);
+    const REAL n_fld = par<ONE>(v.fman, CMF_BATCH_FLOOD_MANNING, v.batched, i, m, M);
+    const REAL elev = v.celv[i];
+    const REAL dx = v.dnd[i];
+    const REAL q_riv_old = v.rout[im];
+    const REAL q_fld_old = v.fout[im];
+    const REAL h_riv = v.rdep[im];
+    const REAL h_fld = v.fdep[im];
+    const REAL hr_before = v.rcsd[im];
+    const REAL hf_before = v.fcsd[im];
+    const REAL af_before = v.fcsa[im];
+    const REAL s_fld = (REAL)fsrc[im];
+
+    // water surfaces: this cell's over its river bed; downstream the next
+    // cell's, or the sea at this catchment's elevation for a mouth
+    const REAL bed = elev - bank_h;
+    const REAL eta = h_riv + bed;
+    const REAL elev_dn = v.celv[dn];
+    const REAL eta_dn = mouth ? elev
+                              : v.rdep[dm] + (elev_dn - par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT,
+                                                                 v.batched, dn, m, M));
+    const REAL eta_top = smax(eta, eta_dn);
+    const REAL slope = (eta - eta_dn) / dx;
+
+    // interface state: river flow depth (the own depth at a mouth, whose sea
+    // level sets the slope only), floodplain flow depth and flow area
+    const REAL hr_now = mouth ? h_riv : eta_top - bed;
+    const REAL hf_now = smax((mouth ? eta : eta_top) - elev, REAL(0));
+    const REAL af_now = smax(s_fld / len - h_fld * width, REAL(0));
+    const REAL hr_si = implicit_mean(hr_now, hr_before, REAL(1e-6));
+    const REAL hf_si = implicit_mean(hf_now, hf_before, REAL(1e-6));
+
+    REAL q_riv = REAL(0);
+    if (hr_si > REAL(1e-5) && hr_now * width > REAL(1e-5))
+        q_riv = channel_discharge(q_riv_old, width, n_riv, hr_si, slope, gdt);
+    REAL q_fld = REAL(0);
+    if (hf_si > REAL(1e-5) && af_now > REAL(1e-5)) {
+        const REAL af_si = implicit_mean(af_now, smax(af_before, REAL(1e-6)), REAL(1e-6));
+        q_fld = plain_discharge(q_fld_old, af_si, n_fld, hf_si, capped_slope(slope, REAL(0.005)), gdt);
+    }
+    // the floodplain never flows against the river
+    if (q_riv * q_fld < REAL(0)) q_fld = REAL(0);
+
+    // river storage, read only where a rule below needs it
+    REAL s_riv = REAL(0);
+    bool have_s_riv = false;
+    auto river_store = [&]() -> REAL {
+        if (!have_s_riv) {
+            s_riv = (REAL)rsrc[im];
+            have_s_riv = true;
         }
-        ro = fmax(ro, (REAL)0.0);
-        ro = fmin(ro, total / time_step);
-        upd_r_out = ro;
-        upd_f_out = (REAL)0.0;
+        return s_riv;
+    };
+    // backwater into the cell draws at most 5 % of what it holds per sub-step
+    if (q_riv < REAL(0) && !mouth) {
+        const REAL held = river_store() + s_fld + (lev_cell ? (REAL)v.ps[im] : REAL(0));
+        const REAL rate = smin(REAL(0.05) * held / ((-q_riv - q_fld) * dt), REAL(1));
+        q_riv *= rate;
+        q_fld *= rate;
+    }
+    if (RES && (fl & CMF_CELL_DAM_UPSTREAM)) {
+        const REAL bed_slope = smax((elev - elev_dn) / dx, v.min_kin);
+        kinematic_outflow(bed_slope, len, h_riv, h_fld, river_store(), s_fld, width, n_riv, n_fld,
+                          dt, q_riv, q_fld);
+    }
+    if (res_cell) {
+        // the release replaces the routed flux; the limiter gathers fluxes,
+        // so nothing scattered before needs undoing
+        const int slot = v.rslot[i];
+        const DamRule<REAL> rule{v.rcons[slot], v.radj[slot], v.remerg[slot],
+                                 v.rnout[slot], v.raout[slot], v.rfcout[slot]};
+        const REAL inflow = (REAL)v.rti[im] + par<ONE>(v.runoff, CMF_BATCH_RUNOFF, v.batched, i, m, M);
+        q_riv = dam_release(rule, river_store() + s_fld, inflow, dt);
+        q_fld = REAL(0);
     }
 
-    v.qur[im] = upd_r_out;
-    v.quf[im] = upd_f_out;
-    v.rcsd[im] = upd_r_cs_dep;
-    v.fcsd[im] = upd_f_cs_dep;
-    v.fcsa[im] = upd_f_cs_area;
+    v.qur[im] = q_riv;
+    v.quf[im] = q_fld;
+    v.rcsd[im] = hr_now;
+    v.fcsd[im] = hf_now;
+    v.fcsa[im] = af_now;
 
-    if (diag) {
-        if (v.wse) v.wse[im] = wse;
-        if (v.pwse) {
-            REAL pwse = wse;
-            if (lev_cell) pwse = fmin(c_elv + v.pdep[im], wse);
-            v.pwse[im] = pwse;
-        }
+    if (st.diag) {
+        if (v.wse) v.wse[im] = eta;
+        if (v.pwse) v.pwse[im] = lev_cell ? smin(elev + v.pdep[im], eta) : eta;
         if (v.tsto) {
-            REAL tot;
-            if (res_cell) {
-                tot = res_total;
-            } else {
-                if (!rs_loaded) rs = (REAL)rsrc[im];
-                REAL ps = lev_cell ? (REAL)v.ps[im] : (REAL)0;
-                tot = rs + fs + ps;
-            }
-            v.tsto[im] = (double)tot;
+            const REAL held = res_cell ? river_store() + s_fld
+                                       : river_store() + s_fld + (lev_cell ? (REAL)v.ps[im] : REAL(0));
+            v.tsto[im] = (double)held;
         }
     }
 }
 
-// Water-surface elevation, protected WSE and total storage of a path end
-// (the values outflow.cu/reservoir.cu leave in the scratch fields).
+// ---------------------------------------------------------------------------
+// k_momentum, path part: the level fluxes of a bifurcation path and its
+// limiter (bifurcation.cu:21-129, levee.cu:263-341), from cmf_physics.cuh.
+// ---------------------------------------------------------------------------
+
+// The end-cell quantities a path reads: water-surface elevation, protected
+// water surface (the levee's crown side, capped by the river surface) and
+// total storage -- what the reference's outflow and reservoir kernels leave
+// in its scratch fields.
 template <typename REAL, bool ONE, bool RES, bool LEV>
 __device__ __forceinline__ void path_end_state(const Dev<REAL>& v, const double* rsrc,
-                                               const double* fsrc, int c, int m, REAL& wse,
-                                               REAL& pwse, REAL& tot)
+                                               const double* fsrc, int c, int m, REAL& eta,
+                                               REAL& peta, REAL& store)
 {
     const long cm = ix<ONE>(c, m, v.M);
     const uint8_t fl = v.flags[c];
-    REAL r_dep = v.rdep[cm];
-    REAL r_hgt = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, c, m, v.M);
-    REAL c_elv = v.celv[c];
-    wse = r_dep + (c_elv - r_hgt);
-    pwse = wse;
+    const REAL elev = v.celv[c];
+    eta = v.rdep[cm] + (elev - par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, c, m, v.M));
     const bool lev_cell = LEV && (fl & CMF_CELL_LEVEE);
-    if (lev_cell) pwse = fmin(c_elv + v.pdep[cm], wse);
-    REAL rs = (REAL)rsrc[cm];
-    REAL fs = (REAL)fsrc[cm];
-    if (RES && (fl & CMF_CELL_RESERVOIR)) {
-        tot = rs + fs;
-    } else {
-        REAL ps = lev_cell ? (REAL)v.ps[cm] : (REAL)0;
-        tot = rs + fs + ps;
-    }
+    peta = lev_cell ? smin(elev + v.pdep[cm], eta) : eta;
+    const REAL held = (REAL)rsrc[cm] + (REAL)fsrc[cm];
+    store = (RES && (fl & CMF_CELL_RESERVOIR)) ? held
+                                               : held + (lev_cell ? (REAL)v.ps[cm] : REAL(0));
 }
 
-// ---------------------------------------------------------------------------
-// k_momentum: path part (bifurcation.cu:21-129, levee.cu:263-341)
-// ---------------------------------------------------------------------------
+// Level fields of path p for member m, loaded on first use.
+template <typename REAL, bool ONE>
+struct PathLevelFields {
+    const Dev<REAL>& v;
+    long p;
+    int m;
+    __device__ long par_at(int l) const { return p * (long)v.L + l; }
+    __device__ long state_at(int l) const { return ix<ONE>(par_at(l), m, v.M); }
+    __device__ REAL sill(int l) const { return v.belv[par_at(l)]; }
+    __device__ REAL width(int l) const { return v.bwid[par_at(l)]; }
+    __device__ REAL manning(int l) const { return v.bman[par_at(l)]; }
+    __device__ REAL flux(int l) const { return v.bout[state_at(l)]; }
+    __device__ REAL depth(int l) const { return v.bcsd[state_at(l)]; }
+    __device__ void new_depth(int l, REAL h) const { v.bcsd[state_at(l)] = h; }
+};
+
 template <typename REAL, bool ONE, bool RES, bool LEV>
 __device__ __forceinline__ void momentum_path(const Dev<REAL>& v, long p, int m, int kh)
 {
     const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
     if (!st.active) return;
-    const int k = st.k;
-    const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
-    const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
-    const int M = v.M;
-    const int L = v.L;
-    const REAL time_step = v.dt[m];
-    const REAL gravity = v.g;
-    const int ci = v.bci[p];
-    const int di = v.bdi[p];
-    const REAL blen = v.blen[p];
-    REAL wse_c, pwse_c, ts_c, wse_d, pwse_d, ts_d;
-    path_end_state<REAL, ONE, RES, LEV>(v, rsrc, fsrc, ci, m, wse_c, pwse_c, ts_c);
-    path_end_state<REAL, ONE, RES, LEV>(v, rsrc, fsrc, di, m, wse_d, pwse_d, ts_d);
-    REAL max_wse = fmax(wse_c, wse_d);
-    REAL max_pwse = fmax(pwse_c, pwse_d);
-    REAL slope = (wse_c - wse_d) / blen;
-    slope = fmin(fmax(slope, (REAL)-0.005), (REAL)0.005);
-
-    REAL upd[kMaxBifLevels];
-    REAL sum_out = (REAL)0;
+    const double* rsrc = (st.k & 1) ? v.rs1 : v.rs0;
+    const double* fsrc = (st.k & 1) ? v.fs1 : v.fs0;
+    const REAL dt = v.dt[m];
+    PathEnds<REAL> ends;
+    path_end_state<REAL, ONE, RES, LEV>(v, rsrc, fsrc, v.bci[p], m, ends.eta_a, ends.peta_a,
+                                        ends.store_a);
+    path_end_state<REAL, ONE, RES, LEV>(v, rsrc, fsrc, v.bdi[p], m, ends.eta_b, ends.peta_b,
+                                        ends.store_b);
+    const PathLevelFields<REAL, ONE> lv{v, p, m};
+    REAL flux[kMaxBifLevels];
+    const REAL sum = path_level_fluxes<LEV>(lv, v.L, ends, v.blen[p], v.g * dt, flux);
+    const REAL rate = path_rate(sum, ends.store_a, ends.store_b, dt);
+    REAL moved = REAL(0);
 #pragma unroll
-    for (int lv = 0; lv < kMaxBifLevels; ++lv) {
-        REAL upd_o = (REAL)0;
-        if (lv < L) {
-            const long lp = p * (long)L + lv;      // parameter index
-            const long ls = ix<ONE>(lp, m, M);     // state index
-            REAL elv = v.belv[lp];
-            REAL upd_csd;
-            REAL sifd;
-            if (LEV) {
-                REAL current_max_wse = (lv == 0) ? max_wse : max_pwse;
-                upd_csd = fmax(current_max_wse - elv, (REAL)0.0);
-                if (lv == 0) {
-                    REAL old_csd = v.bcsd[ls];
-                    sifd = sqrt(upd_csd * old_csd);
-                    if (sifd <= (REAL)0.0) sifd = upd_csd;
-                } else {
-                    sifd = upd_csd;
-                }
-            } else {
-                REAL csd = v.bcsd[ls];
-                upd_csd = fmax(max_wse - elv, (REAL)0);
-                sifd = fmax(sqrt(upd_csd * csd), sqrt(upd_csd * (REAL)0.01));
-            }
-            if (sifd > (REAL)1e-5) {
-                REAL man = v.bman[lp];
-                REAL w = v.bwid[lp];
-                REAL o = v.bout[ls];
-                REAL unit_o = o / w;
-                REAL num = w * (unit_o + gravity * time_step * sifd * slope);
-                REAL den = (REAL)1 + gravity * time_step * (man * man) * fabs(unit_o)
-                           * ((REAL)1 / pow73(sifd));
-                upd_o = num / den;
-            }
-            sum_out += upd_o;
-            v.bcsd[ls] = upd_csd;
-        }
-        upd[lv] = upd_o;
-    }
-    REAL limit_rate = fmin((REAL)0.05 * fmin(ts_c, ts_d) / (fabs(sum_out) * time_step), (REAL)1);
-    sum_out *= limit_rate;
-    REAL raw = (REAL)0;
-#pragma unroll
-    for (int lv = 0; lv < kMaxBifLevels; ++lv) {
-        if (lv < L) {
-            REAL o = upd[lv] * limit_rate;
-            v.bout[ix<ONE>(p * (long)L + lv, m, M)] = o;
-            raw += o;
+    for (int l = 0; l < kMaxBifLevels; ++l) {
+        if (l < v.L) {
+            const REAL q = flux[l] * rate;
+            v.bout[lv.state_at(l)] = q;
+            moved += q;
         }
     }
-    const long pm = ix<ONE>(p, m, M);
-    v.bsum[pm] = sum_out;
-    v.braw[pm] = raw;
+    const long pm = ix<ONE>(p, m, v.M);
+    v.bsum[pm] = sum * rate;
+    v.braw[pm] = moved;
 }
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF>
@@ -604,284 +505,51 @@ __device__ __forceinline__ REAL limit_rate_of(const Dev<REAL>& v, const double* 
 }
 
 // ---------------------------------------------------------------------------
-// Flood stage (storage.cu:118-211) on a known total storage.  Writes river /
-// flood storage split, depths and fraction into the out-parameters.
+// A catchment's floodplain profile for the flood stage: the catchment area
+// and the table row, needed only by cells above their banks.  The CaMa layout
+// (kRowRegs levels) keeps the row in registers; stage_cell starts its loads
+// early for cells that were flooded before the sub-step.  Other level counts
+// walk the row in memory.
 // ---------------------------------------------------------------------------
 template <typename REAL>
-struct StageOut {
-    double rs, fs;
-    REAL rdep, fdep, ffr;
-};
-
-// A floodplain-table row held in registers (the CaMa layout has exactly
-// kRowRegs levels; other level counts scan the row from memory) together with
-// the catchment area, both needed only by flooded cells.
-template <typename REAL>
-struct TableRow {
-    REAL H[kRowRegs];
+struct CellProfile {
+    const Dev<REAL>* v;
+    long i;
+    REAL D[kRowRegs];
     REAL ca;
-    bool valid;
-};
+    bool loaded;
 
-// Issue the row loads (independent 8-byte loads for fp32) and the area load.
-template <typename REAL>
-__device__ __forceinline__ void load_row(const Dev<REAL>& v, long i, TableRow<REAL>& r)
-{
-    const REAL* __restrict__ row = v.tbl + i * (long)kRowRegs;
-    if (sizeof(REAL) == 4 && ((uintptr_t)row & 7) == 0) {
-        const float2* r2 = reinterpret_cast<const float2*>(row);
+    __device__ void load()
+    {
+        const REAL* __restrict__ row = v->tbl + i * (long)kRowRegs;
+        if (sizeof(REAL) == 4 && ((uintptr_t)row & 7) == 0) {
+            const float2* r2 = reinterpret_cast<const float2*>(row);
 #pragma unroll
-        for (int q = 0; q < kRowRegs / 2; ++q) {
-            float2 x = __ldg(r2 + q);
-            r.H[2 * q] = (REAL)x.x;
-            r.H[2 * q + 1] = (REAL)x.y;
-        }
-    } else {
-#pragma unroll
-        for (int l = 0; l < kRowRegs; ++l) r.H[l] = __ldg(row + l);
-    }
-    r.ca = v.ca[i];
-    r.valid = true;
-}
-
-template <typename REAL, bool ONE>
-__device__ __forceinline__ void flood_stage(const Dev<REAL>& v, long i, int m, double total_s,
-                                            REAL rh, REAL rw, REAL rl, TableRow<REAL>& row,
-                                            StageOut<REAL>& o)
-{
-    REAL total_storage = (REAL)total_s;
-    REAL river_max_storage = rl * rw * rh;
-    if (total_storage <= river_max_storage) {
-        o.rs = total_s;
-        o.fs = 0.0;
-        o.rdep = total_storage / (rl * rw);
-        o.fdep = (REAL)0;
-        o.ffr = (REAL)0;
-        return;
-    }
-    const int nl = v.K;
-    const bool in_regs = nl == kRowRegs;
-    if (in_regs && !row.valid) load_row(v, i, row);
-    REAL ca = in_regs ? row.ca : v.ca[i];
-    REAL catchment_width = ca / rl;
-    REAL width_increment = catchment_width / (REAL)nl;
-    int level = 0;
-    REAL S_accum = river_max_storage;
-    REAL prev_H = (REAL)0;
-    REAL prev_W = rw;
-    REAL prev_total_storage = river_max_storage;
-    REAL prev_flood_depth = (REAL)0;
-    REAL next_flood_depth = (REAL)0;
-    // The scan stops at the first level the storage does not exceed, exactly
-    // as the reference's `break`.
-    auto level_step = [&](int l, REAL H_curr) -> bool {
-        REAL W_curr = rw + (REAL)(l + 1) * width_increment;
-        REAL dS = rl * (REAL)0.5 * (prev_W + W_curr) * (H_curr - prev_H);
-        REAL S_curr = S_accum + dS;
-        next_flood_depth = H_curr;
-        if (total_storage > S_curr) {
-            level += 1;
-            prev_total_storage = S_curr;
-            prev_flood_depth = H_curr;
-            S_accum = S_curr;
-            prev_H = H_curr;
-            prev_W = W_curr;
-            return true;
-        }
-        return false;
-    };
-    if (in_regs) {
-        // row loaded up front (independent loads, one memory latency)
-        bool scanning = true;
-#pragma unroll
-        for (int l = 0; l < kRowRegs; ++l)
-            if (scanning) scanning = level_step(l, row.H[l]);
-    } else {
-        const REAL* trow = v.tbl + i * (long)nl;
-        for (int l = 0; l < nl; ++l)
-            if (!level_step(l, __ldg(trow + l))) break;
-    }
-    REAL prev_total_width = rw + (REAL)level * width_increment;
-    REAL diff_width = (REAL)0;
-    REAL fdep;
-    if (level == nl) {
-        fdep = prev_flood_depth + (total_storage - prev_total_storage) / (prev_total_width * rl);
-    } else {
-        REAL flood_grad = (next_flood_depth - prev_flood_depth) / width_increment;
-        diff_width = sqrt(prev_total_width * prev_total_width
-                          + (REAL)2 * (total_storage - prev_total_storage) / (flood_grad * rl))
-                     - prev_total_width;
-        fdep = prev_flood_depth + diff_width * flood_grad;
-    }
-    REAL cap = river_max_storage + rl * rw * fdep;
-    double cap_s = (double)cap;
-    double river_storage_final = cap_s < total_s ? cap_s : total_s;
-    REAL rdep = (REAL)river_storage_final / (rl * rw);
-    REAL ff_mid = (prev_total_width + diff_width - rw) * rl / ca;
-    ff_mid = ff_mid < (REAL)0 ? (REAL)0 : (ff_mid > (REAL)1 ? (REAL)1 : ff_mid);
-    REAL ffr = (level == nl) ? (REAL)1 : ff_mid;
-    double flood_storage_final = total_s - river_storage_final;
-    if (flood_storage_final < 0.0) flood_storage_final = 0.0;
-    o.rs = river_storage_final;
-    o.fs = flood_storage_final;
-    o.rdep = rdep;
-    o.fdep = fdep;
-    o.ffr = ffr;
-}
-
-// ---------------------------------------------------------------------------
-// Levee re-partition (levee.cu:29-261) of one levee cell after its flood
-// stage.  In: storages/depths/fraction from flood_stage.  Out: the same plus
-// protected storage/depth.
-// ---------------------------------------------------------------------------
-template <typename REAL>
-__device__ __forceinline__ REAL clamp01(REAL x) { return fmin(fmax(x, (REAL)0), (REAL)1); }
-
-template <typename REAL, bool ONE>
-__device__ __forceinline__ void levee_stage(const Dev<REAL>& v, const REAL* row, REAL l_crown,
-                                            REAL l_frac, REAL l_base_h, REAL ca, REAL rh,
-                                            REAL rw, REAL rl, StageOut<REAL>& s, double& p_out,
-                                            REAL& pdep_out)
-{
-    const int nl = v.K;
-    double riv_sto_curr_hp = s.rs;
-    double fld_sto_curr_hp = s.fs;
-    double total_sto_hp = riv_sto_curr_hp + fld_sto_curr_hp;
-    REAL riv_sto_curr = (REAL)riv_sto_curr_hp;
-    REAL fld_sto_curr = (REAL)fld_sto_curr_hp;
-    REAL fld_depth_curr = s.fdep;
-    REAL total_sto = (REAL)total_sto_hp;
-    REAL riv_max_sto = rl * rw * rh;
-    if (!(total_sto >= riv_max_sto)) {
-        p_out = 0.0;
-        pdep_out = (REAL)0.0;
-        return;
-    }
-    REAL dwth_inc = (ca / rl) / (REAL)nl;
-    REAL levee_dist = l_frac * (ca / rl);
-    REAL s_curr = riv_max_sto;
-    REAL dhgt_pre = (REAL)0.0;
-    REAL dwth_pre = rw;
-    REAL levee_base_sto = riv_max_sto;
-    REAL levee_fill_sto = riv_max_sto;
-    bool found_base = false, found_fill = false;
-    int ilev = (int)(l_frac * (REAL)nl);
-    REAL dsto_fil_B = (REAL)0.0, dwth_fil_B = (REAL)0.0, ddph_fil_B = (REAL)0.0,
-         gradient_B = (REAL)0.0;
-    bool found_B = false;
-    bool scan_needed = true;
-    for (int l = 0; l < nl; ++l) {
-        if (!scan_needed) break;
-        REAL depth_val = row[l];
-        REAL dhgt_seg = fmax(depth_val - dhgt_pre, (REAL)1e-6);
-        REAL dwth_mid = dwth_pre + (REAL)0.5 * dwth_inc;
-        REAL dsto_seg = rl * dwth_mid * dhgt_seg;
-        REAL s_next = s_curr + dsto_seg;
-        REAL gradient = dhgt_seg / dwth_inc;
-
-        bool cond_base = (l_base_h > dhgt_pre) && (l_base_h <= depth_val);
-        REAL ratio_base = (l_base_h - dhgt_pre) / dhgt_seg;
-        REAL dsto_base_p = rl * (dwth_pre + (REAL)0.5 * ratio_base * dwth_inc) * (ratio_base * dhgt_seg);
-        if (cond_base && !found_base) levee_base_sto = s_curr + dsto_base_p;
-        found_base = found_base || cond_base;
-
-        bool cond_fill = (l_crown > dhgt_pre) && (l_crown <= depth_val);
-        REAL ratio_fill = (l_crown - dhgt_pre) / dhgt_seg;
-        REAL dsto_fill_p = rl * (dwth_pre + (REAL)0.5 * ratio_fill * dwth_inc) * (ratio_fill * dhgt_seg);
-        if (cond_fill && !found_fill) levee_fill_sto = s_curr + dsto_fill_p;
-        found_fill = found_fill || cond_fill;
-
-        REAL dhgt_dif_loop = l_crown - l_base_h;
-        REAL s_top_loop = levee_base_sto + (levee_dist + rw) * dhgt_dif_loop * rl;
-        REAL dsto_add_wedge = (levee_dist + rw) * (l_crown - depth_val) * rl;
-        REAL threshold = s_next + dsto_add_wedge;
-
-        bool cond_check = (l >= ilev) && !found_B;
-        bool cond_found = cond_check && (total_sto < threshold);
-        REAL current_lb = (l == ilev) ? s_top_loop : dsto_fil_B;
-        if (cond_check && !cond_found) {
-            dsto_fil_B = threshold;
-            dwth_fil_B = dwth_inc * (REAL)(l + 1) - levee_dist;
-            ddph_fil_B = depth_val - l_base_h;
+            for (int q = 0; q < kRowRegs / 2; ++q) {
+                const float2 x = __ldg(r2 + q);
+                D[2 * q] = (REAL)x.x;
+                D[2 * q + 1] = (REAL)x.y;
+            }
         } else {
-            dsto_fil_B = current_lb;
+#pragma unroll
+            for (int l = 0; l < kRowRegs; ++l) D[l] = __ldg(row + l);
         }
-        if (cond_found) gradient_B = gradient;
-        found_B = found_B || cond_found;
-
-        s_curr = s_next;
-        dhgt_pre = depth_val;
-        dwth_pre += dwth_inc;
-        scan_needed = !(found_base && found_fill && found_B);
+        ca = v->ca[i];
+        loaded = true;
     }
-    REAL s_base_extra = s_curr + rl * dwth_pre * (l_base_h - dhgt_pre);
-    if (!found_base) levee_base_sto = (l_base_h > dhgt_pre) ? s_base_extra : riv_max_sto;
-    REAL s_fill_extra = s_curr + rl * dwth_pre * (l_crown - dhgt_pre);
-    if (!found_fill) levee_fill_sto = (l_crown > dhgt_pre) ? s_fill_extra : riv_max_sto;
-
-    REAL dhgt_dif = l_crown - l_base_h;
-    REAL s_top = levee_base_sto + (levee_dist + rw) * dhgt_dif * rl;
-    bool is_case4 = total_sto >= levee_fill_sto;
-    bool is_case3 = (!is_case4) && (total_sto >= s_top);
-    bool is_case2 = (!is_case4) && (!is_case3) && (total_sto >= levee_base_sto);
-
-    REAL dsto_add_c2 = total_sto - levee_base_sto;
-    REAL dwth_add_c2 = levee_dist + rw;
-    REAL f_dph_c2 = l_base_h + dsto_add_c2 / dwth_add_c2 / rl;
-    REAL r_sto_c2 = riv_max_sto + rl * rw * f_dph_c2;
-    REAL r_dph_c2 = r_sto_c2 / rl / rw;
-    REAL f_sto_c2 = fmax(total_sto - r_sto_c2, (REAL)0.0);
-    REAL f_frc_c2 = l_frac;
-
-    REAL dsto_add_B = total_sto - dsto_fil_B;
-    REAL term_B = dwth_fil_B * dwth_fil_B + (REAL)2.0 * dsto_add_B / rl / (gradient_B + (REAL)1e-9);
-    REAL dwth_add_B = -dwth_fil_B + sqrt(fmax(term_B, (REAL)0.0));
-    REAL ddph_add_B = dwth_add_B * gradient_B;
-    REAL p_dph_B_found = l_base_h + ddph_fil_B + ddph_add_B;
-    REAL f_frc_B_found = (dwth_fil_B + levee_dist) / (dwth_inc * (REAL)nl);
-    REAL ddph_add_B_extra = dsto_add_B / (dwth_fil_B * rl + (REAL)1e-9);
-    REAL p_dph_B_extra = l_base_h + ddph_fil_B + ddph_add_B_extra;
-    REAL p_dph_B = found_B ? p_dph_B_found : p_dph_B_extra;
-    REAL f_frc_B = found_B ? f_frc_B_found : (REAL)1.0;
-
-    REAL f_dph_c3 = l_crown;
-    REAL r_sto_c3 = riv_max_sto + rl * rw * f_dph_c3;
-    REAL r_dph_c3 = r_sto_c3 / rl / rw;
-    REAL f_sto_c3 = fmax(s_top - r_sto_c3, (REAL)0.0);
-    REAL p_dph_c3 = p_dph_B;
-    REAL f_frc_c3 = clamp01(f_frc_B);
-
-    REAL f_dph_c4 = fld_depth_curr;
-    REAL r_sto_c4 = riv_sto_curr;
-    REAL dsto_add_c4 = (f_dph_c4 - l_crown) * (levee_dist + rw) * rl;
-    REAL f_sto_c4 = fmax(s_top + dsto_add_c4 - r_sto_c4, (REAL)0.0);
-    REAL p_dph_c4 = f_dph_c4;
-
-    REAL r_sto_candidate = is_case2 ? r_sto_c2 : (is_case3 ? r_sto_c3 : (is_case4 ? r_sto_c4 : riv_sto_curr));
-    REAL f_sto_candidate = is_case2 ? f_sto_c2 : (is_case3 ? f_sto_c3 : (is_case4 ? f_sto_c4 : fld_sto_curr));
-    bool no_levee_partition = !is_case2 && !is_case3 && !is_case4;
-    double r_sto = (is_case4 || no_levee_partition) ? riv_sto_curr_hp
-                                                     : fmin((double)r_sto_candidate, total_sto_hp);
-    double remaining_sto = total_sto_hp - r_sto;
-    remaining_sto = remaining_sto > 0.0 ? remaining_sto : 0.0;
-    double f_sto_candidate_hp = (double)f_sto_candidate;
-    double f_sto = fmin(f_sto_candidate_hp > 0.0 ? f_sto_candidate_hp : 0.0, remaining_sto);
-    if (is_case2) f_sto = remaining_sto;
-    if (no_levee_partition) f_sto = fld_sto_curr_hp;
-    double p_sto = remaining_sto - f_sto;
-    p_sto = p_sto > 0.0 ? p_sto : 0.0;
-    REAL r_dph = is_case2 ? r_dph_c2 : (is_case3 ? r_dph_c3 : s.rdep);
-    REAL f_dph = is_case2 ? f_dph_c2 : (is_case3 ? f_dph_c3 : fld_depth_curr);
-    REAL p_dph = is_case2 ? (REAL)0.0 : (is_case3 ? p_dph_c3 : (is_case4 ? p_dph_c4 : (REAL)0.0));
-    REAL f_frc = is_case2 ? f_frc_c2 : (is_case3 ? f_frc_c3 : s.ffr);
-    s.rs = r_sto;
-    s.fs = f_sto;
-    s.rdep = r_dph;
-    s.fdep = f_dph;
-    s.ffr = f_frc;
-    p_out = p_sto;
-    pdep_out = p_dph;
-}
+    __device__ bool in_regs() const { return v->K == kRowRegs; }
+    __device__ REAL area()
+    {
+        if (!in_regs()) return v->ca[i];
+        if (!loaded) load();
+        return ca;
+    }
+    __device__ FillLevel<REAL> walk(REAL S, REAL bank, REAL width, REAL len, REAL dw)
+    {
+        if (in_regs()) return fill_level_regs(D, S, bank, width, len, dw);
+        return fill_level_mem(v->tbl + i * (long)v->K, v->K, S, bank, width, len, dw);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // Deterministic block sum of kBudgetTerms fp64 values into bpart[term][block]
@@ -954,9 +622,11 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     // A cell flooded in the previous sub-step will almost surely need its
     // floodplain row: start those loads now, alongside the upstream gather.
-    TableRow<REAL> row;
-    row.valid = false;
-    if (v.K == kRowRegs && fsto > 0.0) load_row(v, i, row);
+    CellProfile<REAL> prof;
+    prof.v = &v;
+    prof.i = i;
+    prof.loaded = false;
+    if (v.K == kRowRegs && fsto > 0.0) prof.load();
 
     // upstream inflow: gather the limited fluxes of the upstream cells, in
     // range order, kChildUnroll independent loads at a time
@@ -1008,39 +678,23 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
         }
     }
 
-    // storage update (storage.cu:67-116)
-    const REAL rinf = (REAL)rin;
-    const REAL finf = (REAL)fin;
-    const REAL gbif = BIF ? (REAL)gb : (REAL)0;
-    REAL river_delta = (rinf - rout) * ts;
-    double river_su = rsto + (double)river_delta;
-    REAL flood_delta = (finf - fout - gbif) * ts;
-    double flood_su = fsto + (river_su < 0.0 ? river_su : 0.0) + (double)flood_delta;
-    river_su = river_su > 0.0 ? river_su : 0.0;
-    if (flood_su < 0.0) {
-        double tt = river_su + flood_su;
-        river_su = tt > 0.0 ? tt : 0.0;
-    }
-    flood_su = flood_su > 0.0 ? flood_su : 0.0;
-    REAL external_delta = ro * ts;
-    double total_next = river_su + flood_su + prot + (double)external_delta;
-    double total_s = total_next > 0.0 ? total_next : 0.0;
-
-    StageOut<REAL> s;
-    flood_stage<REAL, ONE>(v, i, m, total_s, rh, rw, rl, row, s);
-    // Levee cells are re-partitioned afterwards by k_levee; the partition
-    // conserves r + f + p, so the budget's end storage is taken here.
-    const double p_new = 0.0;
+    // continuity and flood stage; levee cells are re-partitioned afterwards
+    // by k_levee, which conserves river + flood + protected storage, so the
+    // budget's end storage is taken here
+    const Continuity<double, REAL> c =
+        continuity<double, REAL>(rsto, fsto, prot, (REAL)rin, rout, (REAL)fin, fout,
+                                 BIF ? (REAL)gb : REAL(0), ro, ts);
+    const StageOut<double, REAL> s = flood_stage_of(c.total, rw, rl, rh, v.K, prof);
 
     if (BUDGET) {
         const double pre = rsto + fsto + prot;
-        const double raw_next = rsto + (double)river_delta + fsto + (double)flood_delta + prot
-                                + (double)external_delta;
-        bud[CMF_BUDGET_RUNOFF_IN] += (double)external_delta;
-        bud[CMF_BUDGET_CLIP_GAIN] += total_s - raw_next;
+        const double raw_next = rsto + (double)c.d_river + fsto + (double)c.d_flood + prot
+                                + (double)c.d_runoff;
+        bud[CMF_BUDGET_RUNOFF_IN] += (double)c.d_runoff;
+        bud[CMF_BUDGET_CLIP_GAIN] += c.total - raw_next;
         if (mouth) bud[CMF_BUDGET_MOUTH_OUT] += ((double)rout + (double)fout) * (double)ts;
-        if (k == 0 || kh == -2) bud[CMF_BUDGET_STORAGE_START] += pre;
-        if (st.diag) bud[CMF_BUDGET_STORAGE_END] += s.rs + s.fs + p_new;
+        if (st.k == 0 || kh == -2) bud[CMF_BUDGET_STORAGE_START] += pre;
+        if (st.diag) bud[CMF_BUDGET_STORAGE_END] += s.rs + s.fs;
     }
 
     v.rout[im] = rout;
@@ -1147,17 +801,16 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
             double* fdst = (k & 1) ? v.fs0 : v.fs1;
             const long ci = v.lci[li];
             const long cm = ix<ONE>(ci, m, v.M);
-            const REAL l_crown = v.lcrown[li], l_frac = v.lfrac[li], l_base = v.lbase[li];
-            REAL rh, rw, rl, ca;
-            const REAL* row;
-            StageOut<REAL> s;
-            s.rs = rdst[cm];
-            s.fs = fdst[cm];
-            s.rdep = v.rdep[cm];
-            s.fdep = v.fdep[cm];
-            s.ffr = v.ffr[cm];
+            LeveeState<double, REAL> lst;
+            lst.rs = rdst[cm];
+            lst.fs = fdst[cm];
+            lst.rdep = v.rdep[cm];
+            lst.fdep = v.fdep[cm];
+            lst.ffr = v.ffr[cm];
             // static fields from the levee-indexed copies where the plan keeps
             // them (coalesced over the levee list), else from the cells
+            REAL rh, rw, rl, ca;
+            const REAL* row;
             if (v.lpk_ca) {
                 ca = v.lpk_ca[li];
                 row = v.lpk_tbl + li * (long)v.K;
@@ -1174,17 +827,15 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
                 rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
                 rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
             }
-            double p_new;
-            REAL pdep_new;
-            levee_stage<REAL, ONE>(v, row, l_crown, l_frac, l_base, ca, rh, rw, rl, s, p_new,
-                                   pdep_new);
-            rdst[cm] = s.rs;
-            fdst[cm] = s.fs;
-            v.ps[cm] = p_new;
-            v.rdep[cm] = s.rdep;
-            v.fdep[cm] = s.fdep;
-            v.pdep[cm] = pdep_new;
-            v.ffr[cm] = s.ffr;
+            levee_partition(lst, rw, rh, rl, ca, v.lcrown[li], v.lfrac[li], v.lbase[li], v.K,
+                            [row](int l) { return row[l]; });
+            rdst[cm] = lst.rs;
+            fdst[cm] = lst.fs;
+            v.ps[cm] = lst.ps;
+            v.rdep[cm] = lst.rdep;
+            v.fdep[cm] = lst.fdep;
+            v.pdep[cm] = lst.pdep;
+            v.ffr[cm] = lst.ffr;
         }
     }
     if (kh == -1 && advance) advance_step(v.ctl, h, 1);

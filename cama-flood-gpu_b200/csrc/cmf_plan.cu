@@ -936,10 +936,17 @@ namespace {
 void* g_noalloc_addr[kNoAllocMaxDevices];
 std::mutex g_noalloc_mutex;
 
-int noalloc_scratch(void** out)
+int noalloc_scratch(void* stream, void** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return CMF_ERR_CUDA;
+    // the kernels run on the stream's device and must get that device's
+    // copy of the array: a stream of another device is an argument error
+    if (stream) {
+        int sdev = -1;
+        if (cudaStreamGetDevice((cudaStream_t)stream, &sdev) != cudaSuccess) return CMF_ERR_ARG;
+        if (sdev != dev) return CMF_ERR_ARG;
+    }
     if (dev < 0 || dev >= kNoAllocMaxDevices) return CMF_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_addr[dev]) {
@@ -960,7 +967,7 @@ extern "C" int cmf_substep_noalloc(const CmfView* view, void* stream, int diag)
     if ((view->features & CMF_FEAT_BIFURCATION) && view->num_bifurcation_paths > kNoAllocMaxPaths)
         return CMF_ERR_ARG;
     void* scratch = nullptr;
-    int rc = noalloc_scratch(&scratch);
+    int rc = noalloc_scratch(stream, &scratch);
     if (rc != CMF_OK) return rc;
     CmfView v = *view;
     v.workspace = scratch;

@@ -287,9 +287,11 @@ int cmf_launch_substep(CmfPlan* plan, void* stream, int32_t k, int part);
  * catchments, 8,192 bifurcation paths and one member; larger views return
  * CMF_ERR_ARG.  view.workspace is ignored; view.time_step[0] must hold the
  * sub-step length.  diag != 0 writes the diagnostic fields as
- * cmf_phase_stage does.  The first call on a device looks up the array's
- * device address (with that device current), so make it before any stream
- * capture.  Every call shares the one array: calls that overlap on the GPU
+ * cmf_phase_stage does.  `stream` must belong to the current device (a
+ * stream of another device returns CMF_ERR_ARG): the call uses the current
+ * device's copy of the array.  The first call on a device looks up the
+ * array's device address (with that device current), so make it before any
+ * stream capture.  Every call shares the one array: calls that overlap on the GPU
  * (two streams, two host threads) race and must be serialised by the caller. */
 int cmf_substep_noalloc(const CmfView* view, void* stream, int diag);
 /* Reduce the per-CTA budget partials into view.budget and clear them. */

@@ -98,13 +98,15 @@ def test_interval_bit_exact_vs_reference_cuda(case, device):
 
 
 @needs_ref
-@pytest.mark.parametrize("case", ["full", "res"])
-def test_reference_phase_sequence_bit_exact(case, device):
+@pytest.mark.parametrize("case,log", [("full", False), ("res", False), ("bif", False),
+                                      ("plain", True), ("full", True)])
+def test_reference_phase_sequence_bit_exact(case, log, device):
     """One sub-step driven by the reference's own phase loop
-    (cama_flood_model.py:134-162) through the model's phase callables."""
+    (cama_flood_model.py:134-162) through the model's phase callables; with
+    the log module the loop takes the _log variants."""
     net, orc = _spun_up(case)
     ref = _ref_from_oracle(net, orc)
-    model = P.model_for(net)
+    model = P.model_for(net, budget=log)
     P.load_oracle_state(model, orc)
     r = syn.daily_runoff(net, 6)
     ref.set_runoff(r)
@@ -127,11 +129,20 @@ def test_reference_phase_sequence_bit_exact(case, device):
     model.compute_inflow()
     if bif:
         model.compute_bifurcation_inflow()
-    model.compute_flood_stage()
-    if lev:
-        model.compute_levee_stage()
+    if log:
+        model.compute_flood_stage_log()
+        if lev:
+            model.compute_levee_stage_log()
+        model.flush_budget()
+    else:
+        model.compute_flood_stage()
+        if lev:
+            model.compute_levee_stage()
     torch.cuda.synchronize()
     _assert_bit_exact(model, ref.state(), diag=True)
+    if log:
+        b = model.log.budget.cpu().numpy()
+        assert b[0] > 0 and np.isfinite(b).all(), b
 
 
 @pytest.mark.parametrize("case", list(P.CASES))
