@@ -254,7 +254,7 @@ __device__ __forceinline__ void levee_part(const Ctx& c, long ci, const T* in, G
     st.pdep = T(0);
     st.ffr = T(ffr);
     const double* row = c.tbl + ci * (long)c.K;
-    levee_partition(st, rw, rh, c.rl[ci], c.ca[ci], c.lcrown[slot], c.lfrac[slot], c.lbase[slot],
+    levee_partition<0>(st, rw, rh, c.rl[ci], c.ca[ci], c.lcrown[slot], c.lfrac[slot], c.lbase[slot],
                     c.K, [row](int l) { return row[l]; });
     out[0] = st.rs;
     out[1] = st.fs;

@@ -122,11 +122,13 @@ struct Dev {
     REAL *qur, *quf;
     REAL* lrs;  // limit rate of the current sub-step, per cell x member
     // Levee-indexed copies, packed once per plan (null where the plan keeps
-    // none): each levee cell's catchment area [NLV], floodplain row [NLV][K]
-    // and, when members share them, river height, width, length [3][NLV].
-    REAL* lpk_ca;
+    // none): each levee cell's floodplain row [NLV][K] and, when members
+    // share the river geometry, its river height, width, length [3][NLV] and
+    // the levee's marks (LeveeMarks) [6][NLV]: base, crown, top and
+    // first-layer storages, layer width step, levee distance.
     REAL* lpk_tbl;
     REAL* lpk_geo;
+    REAL* lmk;
 };
 
 // ---------------------------------------------------------------------------
@@ -809,15 +811,9 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
             lst.ffr = v.ffr[cm];
             // static fields from the levee-indexed copies where the plan keeps
             // them (coalesced over the levee list), else from the cells
-            REAL rh, rw, rl, ca;
-            const REAL* row;
-            if (v.lpk_ca) {
-                ca = v.lpk_ca[li];
-                row = v.lpk_tbl + li * (long)v.K;
-            } else {
-                ca = v.ca[ci];
-                row = v.tbl + ci * (long)v.K;
-            }
+            const REAL* row = v.lpk_tbl ? v.lpk_tbl + li * (long)v.K : v.tbl + ci * (long)v.K;
+            auto depth = [row](int l) { return row[l]; };
+            REAL rh, rw, rl;
             if (v.lpk_geo) {
                 rh = v.lpk_geo[li];
                 rw = v.lpk_geo[v.NLV + li];
@@ -827,8 +823,22 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
                 rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
                 rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
             }
-            levee_partition(lst, rw, rh, rl, ca, v.lcrown[li], v.lfrac[li], v.lbase[li], v.K,
-                            [row](int l) { return row[l]; });
+            const REAL crown = v.lcrown[li], frac = v.lfrac[li], base = v.lbase[li];
+            if (v.lmk) {
+                // the plan's marks: the row is read only while the protected
+                // side fills
+                const long n = v.NLV;
+                LeveeMarks<REAL, REAL> mk;
+                mk.s_base = v.lmk[li];
+                mk.s_crown = v.lmk[n + li];
+                mk.s_top = v.lmk[2 * n + li];
+                mk.s_first = v.lmk[3 * n + li];
+                mk.dw = v.lmk[4 * n + li];
+                mk.dist = v.lmk[5 * n + li];
+                levee_apply<0>(lst, mk, rw, rh, rl, crown, frac, base, v.K, depth);
+            } else {
+                levee_partition<0>(lst, rw, rh, rl, v.ca[ci], crown, frac, base, v.K, depth);
+            }
             rdst[cm] = lst.rs;
             fdst[cm] = lst.fs;
             v.ps[cm] = lst.ps;
@@ -994,19 +1004,33 @@ __global__ void __launch_bounds__(256) k_copy_back(const Dev<REAL> v)
     v.fs0[t] = v.fs1[t];
 }
 
-// Levee-indexed copies of the static fields k_levee reads (once per plan).
+// Levee-indexed copies of the static fields k_levee reads, and with a shared
+// river geometry the levees' marks (levee_marks_of on the cell's row), once
+// per plan.
 template <typename REAL>
 __global__ void __launch_bounds__(256) k_levee_pack(const Dev<REAL> v)
 {
     const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= v.NLV) return;
     const long ci = v.lci[l];
-    v.lpk_ca[l] = v.ca[ci];
-    for (int k = 0; k < v.K; ++k) v.lpk_tbl[l * (long)v.K + k] = v.tbl[ci * (long)v.K + k];
+    const REAL* row = v.tbl + ci * (long)v.K;
+    for (int k = 0; k < v.K; ++k) v.lpk_tbl[l * (long)v.K + k] = row[k];
     if (v.lpk_geo) {
         v.lpk_geo[l] = v.rh[ci];
         v.lpk_geo[v.NLV + l] = v.rw[ci];
         v.lpk_geo[2 * v.NLV + l] = v.rl[ci];
+    }
+    if (v.lmk) {
+        const LeveeMarks<REAL, REAL> mk =
+            levee_marks_of<0>(v.rw[ci], v.rh[ci], v.rl[ci], v.ca[ci], v.lcrown[l], v.lfrac[l],
+                              v.lbase[l], v.K, [row](int k) { return row[k]; });
+        const long n = v.NLV;
+        v.lmk[l] = mk.s_base;
+        v.lmk[n + l] = mk.s_crown;
+        v.lmk[2 * n + l] = mk.s_top;
+        v.lmk[3 * n + l] = mk.s_first;
+        v.lmk[4 * n + l] = mk.dw;
+        v.lmk[5 * n + l] = mk.dist;
     }
 }
 

@@ -411,44 +411,6 @@ __device__ __forceinline__ G levee_layer_top(G s_lo, G w_lo, P dh, P dw, P len)
     return xfma(xmul(G(len), xfma(G(P(0.5)), G(dw), w_lo)), G(dh), s_lo);
 }
 
-template <typename G>
-struct LeveeMarks {
-    G s_base, s_crown;
-    int base_layer;  // layer holding the base height (K when not inside the table)
-};
-
-template <typename G, typename P, typename Depth>
-__device__ __forceinline__ LeveeMarks<G> levee_marks(G bank, G width, P len, P dw, int K, P base,
-                                                     P crown, Depth depth_at)
-{
-    LeveeMarks<G> m;
-    m.base_layer = K;
-    bool have_base = false, have_crown = false;
-    G s = bank, w = width;
-    P d = P(0);
-    for (int l = 0; l < K && !(have_base && have_crown); ++l) {
-        const P top = depth_at(l);
-        const P dh = smax(xsub(top, d), P(1e-6));
-        if (!have_base && base > d && base <= top) {
-            m.s_base = levee_partial_storage(s, w, d, dh, dw, len, base);
-            m.base_layer = l;
-            have_base = true;
-        }
-        if (!have_crown && crown > d && crown <= top) {
-            m.s_crown = levee_partial_storage(s, w, d, dh, dw, len, crown);
-            have_crown = true;
-        }
-        s = levee_layer_top(s, w, dh, dw, len);
-        d = top;
-        w = xadd(w, G(dw));
-    }
-    // heights above the table extend the top layer's width vertically; a
-    // height at or below the bank marks the bank
-    if (!have_base) m.s_base = (base > d) ? xfma(xmul(G(len), w), G(xsub(base, d)), s) : bank;
-    if (!have_crown) m.s_crown = (crown > d) ? xfma(xmul(G(len), w), G(xsub(crown, d)), s) : bank;
-    return m;
-}
-
 // Storage that fills the wedge between river and levee from storage s up to
 // the crown, over a surface at height z: s + (d + B) (H_c - z) L.
 template <typename G, typename P>
@@ -457,13 +419,89 @@ __device__ __forceinline__ G wedge_fill(G s, G wedge, P crown, P z, P len)
     return xfma(xmul(wedge, G(xsub(crown, z))), G(len), s);
 }
 
+// Runs fn(l) for the floodplain layers l = 0, 1, ... until fn returns false
+// or the K layers are done.  KR > 0: a row of exactly KR layers held in
+// registers, walked fully unrolled (so that fn may index a register array by
+// l); KR == 0: any K, a plain loop.
+template <int KR, typename Fn>
+__device__ __forceinline__ void for_layers(int K, Fn&& fn)
+{
+    if constexpr (KR > 0) {
+#pragma unroll
+        for (int l = 0; l < KR; ++l)
+            if (!fn(l)) return;
+    } else {
+        for (int l = 0; l < K; ++l)
+            if (!fn(l)) return;
+    }
+}
+
+// What the levee partition needs beyond a cell's flood-stage result: the
+// regime storages of its levee and the layer geometry.  They depend on the
+// river geometry, the floodplain row and the levee alone, so a plan whose
+// geometry is shared by all members computes them once (levee_marks_of) and
+// every sub-step reads them.
+template <typename G, typename P>
+struct LeveeMarks {
+    G s_base;   // profile filled up to the levee base
+    G s_crown;  // profile filled up to the crown
+    G s_top;    // S_base plus the river-side wedge up to the crown
+    G s_first;  // the wedge over the base as the protected-side walk sees it
+                // at its first layer (the base storage once the base layer
+                // is reached, the bank storage before)
+    P dw;       // width step of a layer
+    P dist;     // levee distance from the bank
+};
+
+template <int KR, typename G, typename P, typename Depth>
+__device__ __forceinline__ LeveeMarks<G, P> levee_marks_of(G width, G height, P len, P area,
+                                                           P crown, P frac, P base, int K,
+                                                           Depth depth_at)
+{
+    LeveeMarks<G, P> m;
+    const G bank = xmul(xmul(G(len), width), height);
+    const P span = xdiv(area, len);
+    m.dw = xdiv(span, P(K));
+    m.dist = xmul(frac, span);
+    int base_layer = K;
+    bool have_base = false, have_crown = false;
+    G s = bank, w = width;
+    P d = P(0);
+    for_layers<KR>(K, [&](int l) -> bool {
+        if (have_base && have_crown) return false;
+        const P top = depth_at(l);
+        const P dh = smax(xsub(top, d), P(1e-6));
+        if (!have_base && base > d && base <= top) {
+            m.s_base = levee_partial_storage(s, w, d, dh, m.dw, len, base);
+            base_layer = l;
+            have_base = true;
+        }
+        if (!have_crown && crown > d && crown <= top) {
+            m.s_crown = levee_partial_storage(s, w, d, dh, m.dw, len, crown);
+            have_crown = true;
+        }
+        s = levee_layer_top(s, w, dh, m.dw, len);
+        d = top;
+        w = xadd(w, G(m.dw));
+        return true;
+    });
+    // heights above the table extend the top layer's width vertically; a
+    // height at or below the bank marks the bank
+    if (!have_base) m.s_base = (base > d) ? xfma(xmul(G(len), w), G(xsub(base, d)), s) : bank;
+    if (!have_crown) m.s_crown = (crown > d) ? xfma(xmul(G(len), w), G(xsub(crown, d)), s) : bank;
+    const G wedge = xadd(G(m.dist), width);
+    m.s_top = wedge_fill(m.s_base, wedge, crown, base, len);
+    const int first = (int)xmul(frac, P(K));
+    m.s_first = wedge_fill(base_layer <= first ? m.s_base : bank, wedge, crown, base, len);
+    return m;
+}
+
 // Protected side while the river side stands at the crown.  From layer
 // `first` = floor(frac K) on, the storage that raises the protected surface to
 // the top of layer l is the profile storage there plus the river-side wedge
 // above it up to the crown; the first layer whose threshold exceeds the total
 // storage holds the protected surface; the fill point below it is the
-// previous layer's threshold (at `first` itself: the storage s_first of the
-// wedge filled to the crown over the base as known at that layer).
+// previous layer's threshold (at `first` itself: s_first).
 template <typename G, typename P>
 struct ProtectedFill {
     bool inside;  // the surface lies inside the table
@@ -473,7 +511,7 @@ struct ProtectedFill {
     P grad;       // depth gradient of the layer holding the surface
 };
 
-template <typename G, typename P, typename V, typename Depth>
+template <int KR, typename G, typename P, typename V, typename Depth>
 __device__ __forceinline__ ProtectedFill<G, P> protected_fill(V total, G bank, G width, P len,
                                                               P dw, int K, int first, P crown,
                                                               P base, P dist, G s_first,
@@ -485,7 +523,7 @@ __device__ __forceinline__ ProtectedFill<G, P> protected_fill(V total, G bank, G
     const G wedge = xadd(G(dist), width);
     G s = bank, w = width;
     P d = P(0);
-    for (int l = 0; l < K; ++l) {
+    for_layers<KR>(K, [&](int l) -> bool {
         const P top = depth_at(l);
         const P dh = smax(xsub(top, d), P(1e-6));
         s = levee_layer_top(s, w, dh, dw, len);
@@ -494,7 +532,7 @@ __device__ __forceinline__ ProtectedFill<G, P> protected_fill(V total, G bank, G
             if (val(total) < val(threshold)) {
                 f.inside = true;
                 f.grad = xdiv(dh, dw);
-                return f;
+                return false;
             }
             f.s_fill = threshold;
             f.w_fill = xfma(dw, P(l + 1), -dist);
@@ -502,14 +540,17 @@ __device__ __forceinline__ ProtectedFill<G, P> protected_fill(V total, G bank, G
         }
         d = top;
         w = xadd(w, G(dw));
-    }
+        return true;
+    });
     return f;
 }
 
-template <typename S, typename R, typename G, typename P, typename Depth>
-__device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G height, P len,
-                                                P area, P crown, P frac, P base, int K,
-                                                Depth depth_at)
+// The partition itself, on the levee's marks; the floodplain row is read
+// only when the protected side is filling.
+template <int KR, typename S, typename R, typename G, typename P, typename Depth>
+__device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMarks<G, P>& mk,
+                                            G width, G height, P len, P crown, P frac, P base,
+                                            int K, Depth depth_at)
 {
     const S total_s = st.rs + st.fs;
     const R total = narrow<R>(total_s);
@@ -520,18 +561,12 @@ __device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G
         st.pdep = R(0);
         return;
     }
-    const P span = xdiv(area, len);
-    const P dw = xdiv(span, P(K));
-    const P dist = xmul(frac, span);
-    const G wedge = xadd(G(dist), width);
-    const LeveeMarks<G> mk = levee_marks(bank, width, len, dw, K, base, crown, depth_at);
-    const G s_top = wedge_fill(mk.s_base, wedge, crown, base, len);
-
+    const G wedge = xadd(G(mk.dist), width);
     if (val(total) >= val(mk.s_crown)) {
         // overtopped: river and flood stage stand; the protected side takes
         // what the floodplain holds beyond the wedge at the flood depth
         const S remaining = pos_part(total_s - st.rs);
-        const R at_depth = xfma(xmul(R(xsub(st.fdep, R(crown))), R(wedge)), R(len), R(s_top));
+        const R at_depth = xfma(xmul(R(xsub(st.fdep, R(crown))), R(wedge)), R(len), R(mk.s_top));
         const R outside = smax(xsub(at_depth, narrow<R>(st.rs)), R(0));
         const S fs = smin(pos_part(static_cast<S>(outside)), remaining);
         st.ps = pos_part(remaining - fs);
@@ -539,17 +574,17 @@ __device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G
         st.pdep = st.fdep;
         return;
     }
-    if (val(total) >= val(s_top)) {
+    if (val(total) >= val(mk.s_top)) {
         // river side at the crown, the protected side filling
         const G column = xfma(len_w, G(crown), bank);
         const S rs = smin(static_cast<S>(column), total_s);
         const S remaining = pos_part(total_s - rs);
-        const G outside = smax(xsub(s_top, column), G(0));
+        const G outside = smax(xsub(mk.s_top, column), G(0));
         const S fs = smin(pos_part(static_cast<S>(outside)), remaining);
         const int first = (int)xmul(frac, P(K));
-        const G s_first = wedge_fill(mk.base_layer <= first ? mk.s_base : bank, wedge, crown, base, len);
-        const ProtectedFill<G, P> pf = protected_fill(total, bank, width, len, dw, K, first, crown,
-                                                      base, dist, s_first, depth_at);
+        const ProtectedFill<G, P> pf = protected_fill<KR>(total, bank, width, len, mk.dw, K, first,
+                                                          crown, base, mk.dist, mk.s_first,
+                                                          depth_at);
         const R extra = xsub(total, R(pf.s_fill));
         const P raised = xadd(base, pf.d_fill);
         R pdep, pfrac;
@@ -558,7 +593,7 @@ __device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G
                              xdiv(xdiv(xmul(R(P(2)), extra), R(len)), R(xadd(pf.grad, P(1e-9)))));
             const R w_add = xadd(R(-pf.w_fill), ssqrt(smax(q, R(0))));
             pdep = xadd(R(raised), xmul(w_add, R(pf.grad)));
-            pfrac = R(xdiv(xadd(pf.w_fill, dist), xmul(dw, P(K))));
+            pfrac = R(xdiv(xadd(pf.w_fill, mk.dist), xmul(mk.dw, P(K))));
         } else {
             pdep = xadd(R(raised), xdiv(extra, R(xfma(pf.w_fill, len, P(1e-9)))));
             pfrac = R(1);
@@ -591,6 +626,25 @@ __device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G
     const S remaining = pos_part(total_s - st.rs);
     st.ps = pos_part(remaining - st.fs);
     st.pdep = R(0);
+}
+
+// Marks and partition in one call (geometry that varies by member, the
+// adjoint).  A cell below its banks needs neither.
+template <int KR, typename S, typename R, typename G, typename P, typename Depth>
+__device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G height, P len,
+                                                P area, P crown, P frac, P base, int K,
+                                                Depth depth_at)
+{
+    const R total = narrow<R>(st.rs + st.fs);
+    const G bank = xmul(xmul(G(len), width), height);
+    if (!(val(total) >= val(bank))) {
+        st.ps = S(0);
+        st.pdep = R(0);
+        return;
+    }
+    const LeveeMarks<G, P> mk =
+        levee_marks_of<KR>(width, height, len, area, crown, frac, base, K, depth_at);
+    levee_apply<KR>(st, mk, width, height, len, crown, frac, base, K, depth_at);
 }
 
 }  // namespace cmf

@@ -96,7 +96,7 @@ struct Layout {
     size_t qur, quf, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec;
     size_t base_total;  // the regions every caller needs
     // levee-indexed copies that plans keep (after base_total; none without levees)
-    size_t lpk_ca, lpk_tbl, lpk_geo;
+    size_t lpk_tbl, lpk_geo, lmk;
     size_t total;
 };
 
@@ -119,9 +119,9 @@ Layout layout_of(const CmfView* v, int cell_blocks)
     L.tsec = o; o = align_up(o + 8);
     L.base_total = o;
     const size_t nlv = (v->features & CMF_FEAT_LEVEE) ? (size_t)v->num_levees : 0;
-    L.lpk_ca = o; o = align_up(o + nlv * real);
     L.lpk_tbl = o; o = align_up(o + nlv * (size_t)v->num_flood_levels * real);
     L.lpk_geo = o; o = align_up(o + 3 * nlv * real);
+    L.lmk = o; o = align_up(o + 6 * nlv * real);
     L.total = o;
     return L;
 }
@@ -267,10 +267,12 @@ void fill_dev(CmfPlan* p, const Layout& L, bool packed)
     d.quf = (REAL*)(ws + L.quf);
     d.lrs = (REAL*)(ws + L.lrs);
     if (packed && d.NLV > 0) {
-        d.lpk_ca = (REAL*)(ws + L.lpk_ca);
         d.lpk_tbl = (REAL*)(ws + L.lpk_tbl);
         const int geo = CMF_BATCH_RIVER_HEIGHT | CMF_BATCH_RIVER_WIDTH | CMF_BATCH_RIVER_LENGTH;
-        if (!(v.batched_mask & geo)) d.lpk_geo = (REAL*)(ws + L.lpk_geo);
+        if (!(v.batched_mask & geo)) {
+            d.lpk_geo = (REAL*)(ws + L.lpk_geo);
+            d.lmk = (REAL*)(ws + L.lmk);
+        }
     }
     std::memcpy(p->dev, &d, sizeof(d));
 }
@@ -633,7 +635,8 @@ int cmf_plan_create(const CmfView* view, CmfPlan** out)
         return rc;
     }
     if (p->levee_blocks > 0) {
-        // levee-indexed copies of the static fields k_levee reads
+        // levee-indexed copies of the static fields k_levee reads and, with a
+        // shared river geometry, the levees' marks
         void* args[] = {p->dev};
         const void* fn = p->fp64 ? (const void*)k_levee_pack<double> : (const void*)k_levee_pack<float>;
         rc = launch(fn, ceil_div((long)view->num_levees, 256), 256, args, 0);

@@ -210,14 +210,17 @@ size_t cmf_view_size(void);
 
 /* ---- plan lifecycle ------------------------------------------------------ */
 /* Bytes of scratch the view needs (Qu fluxes, path sums, budget partials,
- * levee-indexed copies of the levee cells' static fields). */
+ * levee-indexed copies of the levee cells' static fields and marks). */
 int cmf_workspace_size(const CmfView* view, size_t* bytes);
 /* Validate the view and bind a plan to its pointers (cmfgpu phys dispatch:
  * BackendRegistry(...).selected binding by parameter name,
  * cmfgpu/phys/outflow.py:51-60).  With levees, the plan copies each levee
- * cell's catchment area, floodplain row and (when not member-batched) river
- * height, width and length into the workspace once, synchronously; a caller
- * that changes those parameters afterwards creates a new plan. */
+ * cell's floodplain row and (when not member-batched) river height, width
+ * and length into the workspace once, synchronously, and with that shared
+ * geometry computes each levee's marks: the storages at which its regimes
+ * change (profile filled to the base and to the crown, the river-side wedge)
+ * and its layer geometry.  A caller that changes those parameters afterwards
+ * creates a new plan. */
 int cmf_plan_create(const CmfView* view, CmfPlan** plan);
 void cmf_plan_destroy(CmfPlan* plan);
 /* Member-tile width of the member-batched kernels (no counterpart in the
