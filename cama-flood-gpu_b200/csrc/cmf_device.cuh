@@ -57,7 +57,16 @@ namespace cmf {
 
 constexpr int kMaxBifLevels = 8;
 constexpr int kRowRegs = 10;         // floodplain levels held in registers (the CaMa layout)
-constexpr int kChildUnroll = 4;      // upstream cells gathered with independent loads
+// Upstream cells gathered with independent loads per loop trip: 4 for one
+// member, whose lanes hold different cells with different upstream counts;
+// 1 with members, where the lanes of a warp row share the cell and a
+// predicated-off trip would only cost issue slots.
+#ifndef CMF_CHILD_UNROLL_BATCHED
+#define CMF_CHILD_UNROLL_BATCHED 1
+#endif
+constexpr int kChildUnroll = 4;
+template <bool ONE>
+__host__ __device__ constexpr int child_unroll() { return ONE ? kChildUnroll : CMF_CHILD_UNROLL_BATCHED; }
 constexpr int kMaxBlock = 256;       // threads per CTA (kernels use __launch_bounds__(256))
 constexpr int kBudgetTerms = CMF_BUDGET_TERMS;
 // control words (Dev::ctl)
@@ -466,10 +475,11 @@ __device__ __forceinline__ REAL outgoing_of(const Dev<REAL>& v, long x, int m, R
     REAL pos = fmax(qr, (REAL)0.0) + fmax(qf, (REAL)0.0);
     double og = (double)(pos * ts);
     const int c0 = v.up[x], c1 = upstream_end(v, x);
-    for (int cb = c0; cb < c1; cb += kChildUnroll) {
-        REAL nr[kChildUnroll], nf[kChildUnroll];
+    constexpr int U = child_unroll<ONE>();
+    for (int cb = c0; cb < c1; cb += U) {
+        REAL nr[U], nf[U];
 #pragma unroll
-        for (int j = 0; j < kChildUnroll; ++j) {
+        for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 const long cm = ix<ONE>(cb + j, m, M);
                 nr[j] = v.qur[cm];
@@ -477,7 +487,7 @@ __device__ __forceinline__ REAL outgoing_of(const Dev<REAL>& v, long x, int m, R
             }
         }
 #pragma unroll
-        for (int j = 0; j < kChildUnroll; ++j) {
+        for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 REAL neg = fmin(nr[j], (REAL)0.0) + fmin(nf[j], (REAL)0.0);
                 og += (double)(-neg * ts);
@@ -631,12 +641,13 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
     if (v.K == kRowRegs && fsto > 0.0) prof.load();
 
     // upstream inflow: gather the limited fluxes of the upstream cells, in
-    // range order, kChildUnroll independent loads at a time
+    // range order, child_unroll independent loads at a time
     double rin = 0.0, fin = 0.0, rti = 0.0;
-    for (int cb = c0; cb < c1; cb += kChildUnroll) {
-        REAL cr[kChildUnroll], cf[kChildUnroll], cl[kChildUnroll];
+    constexpr int U = child_unroll<ONE>();
+    for (int cb = c0; cb < c1; cb += U) {
+        REAL cr[U], cf[U], cl[U];
 #pragma unroll
-        for (int j = 0; j < kChildUnroll; ++j) {
+        for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 const long cm = ix<ONE>(cb + j, m, M);
                 cr[j] = v.qur[cm];
@@ -645,7 +656,7 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
             }
         }
 #pragma unroll
-        for (int j = 0; j < kChildUnroll; ++j) {
+        for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 const REAL ur = (cr[j] >= (REAL)0.0) ? cr[j] * cl[j] : cr[j] * lr_i;
                 const REAL uf = (cf[j] >= (REAL)0.0) ? cf[j] * cl[j] : cf[j] * lr_i;

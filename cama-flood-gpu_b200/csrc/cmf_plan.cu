@@ -347,6 +347,12 @@ int add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* deps
     return check_cuda(cudaGraphAddKernelNode(node, g, deps, ndeps, &kp));
 }
 
+// Dependency edge between two sub-step kernels of the interval graph.
+int add_edge(cudaGraph_t g, cudaGraphNode_t from, cudaGraphNode_t to)
+{
+    return check_cuda(cudaGraphAddDependencies(g, &from, &to, 1));
+}
+
 int build_graph(CmfPlan* p, double T, int fixed_n)
 {
     const CmfView& v = p->view;
@@ -397,18 +403,21 @@ int build_graph(CmfPlan* p, double T, int fixed_n)
         void* a1[] = {p->dev, &kh, &fd};
         if ((rc = add_kernel(&b1, body, nullptr, 0, p->ks.momentum, grid, p->tpb, a1)) != CMF_OK) goto fail;
         void* al[] = {p->dev, &kh};
-        if ((rc = add_kernel(&bl, body, &b1, 1, p->ks.limit, p->cell_blocks, p->tpb, al)) != CMF_OK)
+        if ((rc = add_kernel(&bl, body, nullptr, 0, p->ks.limit, p->cell_blocks, p->tpb, al)) != CMF_OK)
             goto fail;
+        if ((rc = add_edge(body, b1, bl)) != CMF_OK) goto fail;
         int set = 1;
         void* a2[] = {p->dev, &kh, &fd, &h, &set};
-        if ((rc = add_kernel(&b2, body, &bl, 1, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
+        if ((rc = add_kernel(&b2, body, nullptr, 0, p->ks.stage, grid, p->tpb, a2)) != CMF_OK) goto fail;
+        if ((rc = add_edge(body, bl, b2)) != CMF_OK) goto fail;
         cudaGraphNode_t last = b2;
         if (p->levee_blocks > 0) {
             cudaGraphNode_t b3;
             int adv = 1;
             void* a3[] = {p->dev, &kh, &fd, &h, &adv};
-            if ((rc = add_kernel(&b3, body, &b2, 1, p->ks.levee, p->levee_blocks, p->tpb, a3)) != CMF_OK)
+            if ((rc = add_kernel(&b3, body, nullptr, 0, p->ks.levee, p->levee_blocks, p->tpb, a3)) != CMF_OK)
                 goto fail;
+            if ((rc = add_edge(body, b2, b3)) != CMF_OK) goto fail;
             last = b3;
         }
         if (p->stats.count > 0) {
