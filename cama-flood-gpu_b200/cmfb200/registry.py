@@ -49,6 +49,11 @@ class B200Backend:
         adapter takes or returns)."""
         return self.model.base.catchment_id.cpu().numpy()[self.model.inverse_order]
 
+    @property
+    def state_names(self) -> list[str]:
+        """Names of the state tensors the interval step updates."""
+        return list(self.model.state_tensors())
+
     def set_inputs(self, runoff, inflow=None, sea_surface_elevation=None) -> None:
         """Runoff [N] (or [N, M]) in m^3/s, reference catchment order."""
         self.model.set_inputs(runoff, inflow, sea_surface_elevation, order="input")
