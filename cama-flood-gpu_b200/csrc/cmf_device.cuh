@@ -75,6 +75,13 @@ constexpr int kCtlMaxSteps = 1;   // max over members of the sub-step count
 constexpr int kCtlBlocksDone = 2; // last-block-done counter of k_stage
 constexpr int kHardSubStepCap = 100000;  // bound of the device-side sub-step loop
 
+// Two fluxes of one element stored together (river, floodplain): one 8-byte
+// (fp32) or 16-byte (fp64) access instead of two.
+template <typename REAL> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+template <typename REAL> using pair_t = typename Pair<REAL>::type;
+
 template <typename REAL>
 struct Dev {
     long N;
@@ -128,7 +135,7 @@ struct Dev {
     double* bpart;  // [kBudgetTerms][cell_blocks]
     int* status;
     // scratch fluxes
-    REAL *qur, *quf;
+    pair_t<REAL>* qu;  // unlimited (river, floodplain) fluxes
     REAL* lrs;  // limit rate of the current sub-step, per cell x member
     // Levee-indexed copies, packed once per plan (null where the plan keeps
     // none): each levee cell's floodplain row [NLV][K] and, when members
@@ -348,8 +355,7 @@ __device__ __forceinline__ void momentum_cell(const Dev<REAL>& v, long i, int m,
         q_fld = REAL(0);
     }
 
-    v.qur[im] = q_riv;
-    v.quf[im] = q_fld;
+    v.qu[im] = {q_riv, q_fld};
     v.rcsd[im] = hr_now;
     v.fcsd[im] = hf_now;
     v.fcsa[im] = af_now;
@@ -482,8 +488,9 @@ __device__ __forceinline__ REAL outgoing_of(const Dev<REAL>& v, long x, int m, R
         for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 const long cm = ix<ONE>(cb + j, m, M);
-                nr[j] = v.qur[cm];
-                nf[j] = v.quf[cm];
+                const pair_t<REAL> q = v.qu[cm];
+                nr[j] = q.x;
+                nf[j] = q.y;
             }
         }
 #pragma unroll
@@ -511,7 +518,8 @@ __device__ __forceinline__ REAL limit_rate_of(const Dev<REAL>& v, const double* 
                                               const double* fsrc, long x, int m, REAL ts)
 {
     const long xm = ix<ONE>(x, m, v.M);
-    REAL outgoing = outgoing_of<REAL, ONE, BIF>(v, x, m, ts, v.qur[xm], v.quf[xm]);
+    const pair_t<REAL> q = v.qu[xm];
+    REAL outgoing = outgoing_of<REAL, ONE, BIF>(v, x, m, ts, q.x, q.y);
     REAL rate_storage = (REAL)(rsrc[xm] + fsrc[xm]);
     return (outgoing > (REAL)1e-8) ? fmin(rate_storage / outgoing, (REAL)1.0) : (REAL)1.0;
 }
@@ -622,7 +630,8 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     const double rsto = rsrc[im];
     const double fsto = fsrc[im];
-    const REAL qr = v.qur[im], qf = v.quf[im];
+    const pair_t<REAL> q_own = v.qu[im];
+    const REAL qr = q_own.x, qf = q_own.y;
     const REAL ro = par<ONE>(v.runoff, CMF_BATCH_RUNOFF, v.batched, i, m, M);
     const REAL rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, i, m, M);
     const REAL rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, i, m, M);
@@ -650,8 +659,9 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
         for (int j = 0; j < U; ++j) {
             if (cb + j < c1) {
                 const long cm = ix<ONE>(cb + j, m, M);
-                cr[j] = v.qur[cm];
-                cf[j] = v.quf[cm];
+                const pair_t<REAL> q = v.qu[cm];
+                cr[j] = q.x;
+                cf[j] = q.y;
                 cl[j] = v.lrs[cm];
             }
         }

@@ -93,7 +93,7 @@ KernelSet pick_one(bool one, bool res, bool lev, bool bif, bool bud)
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t qur, quf, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec;
+    size_t qu, lrs, bsum, braw, rs1, fs1, bpart, ctl, tsec;
     size_t base_total;  // the regions every caller needs
     // levee-indexed copies that plans keep (after base_total; none without levees)
     size_t lpk_tbl, lpk_geo, lmk;
@@ -107,9 +107,8 @@ Layout layout_of(const CmfView* v, int cell_blocks)
     const size_t pm = (size_t)v->num_bifurcation_paths * (size_t)v->num_members;
     Layout L;
     size_t o = 0;
-    L.qur = o; o = align_up(o + nm * real);
+    L.qu = o; o = align_up(o + 2 * nm * real);
     L.lrs = o; o = align_up(o + nm * real);
-    L.quf = o; o = align_up(o + nm * real);
     L.bsum = o; o = align_up(o + pm * real);
     L.braw = o; o = align_up(o + pm * real);
     L.rs1 = o; o = align_up(o + nm * 8);
@@ -263,8 +262,7 @@ void fill_dev(CmfPlan* p, const Layout& L, bool packed)
     d.budget = v.budget;
     d.bpart = (double*)(ws + L.bpart);
     d.status = v.status;
-    d.qur = (REAL*)(ws + L.qur);
-    d.quf = (REAL*)(ws + L.quf);
+    d.qu = (pair_t<REAL>*)(ws + L.qu);
     d.lrs = (REAL*)(ws + L.lrs);
     if (packed && d.NLV > 0) {
         d.lpk_tbl = (REAL*)(ws + L.lpk_tbl);
