@@ -1110,60 +1110,82 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
     a.scr[S_QFB * N + j] = qf_bar;
 }
 
-// Path momentum reversed (kr_path): one thread per path and input direction
-// (6 end-state inputs and two per level) evaluates one dual pass of the path
-// flux and writes that input's adjoint: lambda_k of the path state, or an
-// end-state adjoint left for the end cell.
-// Path momentum reversed, direction thread t (p = t / (6 + 2L)).  Runs as the
-// trailing blocks of the kr_momentum launch: it reads the tape, the
-// outgoing-storage adjoint of kr_limit and the path buffers of kr_stage_path,
-// and writes only the path lambdas and the path-end buffer, none of which the
-// momentum or dam reverse touches.
+// Path momentum reversed (kr_path): each thread takes kPathLanes of the
+// path's input directions (6 end-state inputs and two per level) and
+// evaluates the path flux once on DualN<kPathLanes> numbers seeded with
+// them, so the primal part of the evaluation (roots, divisions, branches)
+// runs once per kPathLanes directions; it writes each direction's adjoint:
+// lambda_k of the path state, or an end-state adjoint left for the end cell.
+// Runs as the trailing blocks of the kr_momentum launch: it reads the tape,
+// the outgoing-storage adjoint of kr_limit and the path buffers of
+// kr_stage_path, and writes only the path lambdas and the path-end buffer,
+// none of which the momentum or dam reverse touches.  Two lanes: wider
+// numbers spill under the launch's 64-register cap (measured on the 250k
+// full-physics window: 247 us per reverse sub-step at 2 lanes, 253 at 4,
+// 293 at 8, 265 with one direction per thread).
+#ifndef CMF_ADJ_PATH_LANES
+#define CMF_ADJ_PATH_LANES 2
+#endif
+constexpr int kPathLanes = CMF_ADJ_PATH_LANES;
+
+__host__ __device__ constexpr int path_threads(int L) { return (6 + 2 * L + kPathLanes - 1) / kPathLanes; }
+
 __device__ __forceinline__ void path_reverse(const Ctx& c, const double* X, double dt, const Adj& a,
                                              long t)
 {
     const int L = c.L;
     const int NI = 6 + 2 * L;
-    if (t >= c.P * (long)NI) return;
-    const long p = t / NI;
-    const int j = (int)(t - p * NI);
+    const int G = path_threads(L);
+    if (t >= c.P * (long)G) return;
+    const long p = t / G;
+    const int j0 = (int)(t - p * G) * kPathLanes;
     const long N = c.N;
     const int ci = c.bci[p], di = c.bdi[p];
+    using D = DualN<kPathLanes>;
     double in[6 + 2 * kMaxLevels];
     path_inputs(c, X, p, in);
-    Dual x[6 + 2 * kMaxLevels];
-    for (int q = 0; q < NI; ++q) x[q] = {in[q], q == j ? 1.0 : 0.0};
-    Dual blim[kMaxLevels], bcsd_new[kMaxLevels], bs;
-    path_flux<Dual>(c, p, x, dt, blim, bs, bcsd_new);
+    D x[6 + 2 * kMaxLevels];
+    for (int q = 0; q < NI; ++q) {
+        x[q] = D(in[q]);
+        if (q >= j0 && q < j0 + kPathLanes) x[q].d[q - j0] = 1.0;
+    }
+    D blim[kMaxLevels], bcsd_new[kMaxLevels], bs;
+    path_flux<D>(c, p, x, dt, blim, bs, bcsd_new);
     const double bsum = bsum_of(c, X)[p];
     double sb = 0.0;
     if (bsum >= 0.0) sb += a.scr[S_OGB * N + ci] * dt;
     if (bsum <= 0.0) sb -= a.scr[S_OGB * N + di] * dt;
     const double* bb = blimb(c, a.scr);
     const double* cb = bcsdb(c, a.scr);
-    double v = sb * bs.d;
-    for (int lv = 0; lv < L; ++lv) v += bb[p * L + lv] * blim[lv].d + cb[p * L + lv] * bcsd_new[lv].d;
-    if (j >= 6 + L) {
-        lam_path(c, a.lam, PF_BCSD)[p * L + (j - 6 - L)] = v;
-    } else if (j >= 6) {
-        lam_path(c, a.lam, PF_BOUT)[p * L + (j - 6)] = v;
-    } else {
-        // end state: [wse, protected-WSE part on the WSE, protected depth, total storage]
-        const int end = j & 1;
-        double* q = peb(c, a.scr) + 8L * p + 4 * end;
-        if (j < 2) {
-            q[0] = v;
-        } else if (j < 4) {
-            const int e = end ? di : ci;
-            bool to_pdep = false;
-            if (c.lev && (c.flags[e] & CMF_CELL_LEVEE)) {
-                const double wse = X[F_RDEP * N + e] + (c.celv[e] - c.rh[e]);
-                to_pdep = c.celv[e] + X[F_PDEP * N + e] <= wse;
-            }
-            q[1] = to_pdep ? 0.0 : v;
-            q[2] = to_pdep ? v : 0.0;
+#pragma unroll
+    for (int k = 0; k < kPathLanes; ++k) {
+        const int j = j0 + k;
+        if (j >= NI) break;
+        double v = sb * bs.d[k];
+        for (int lv = 0; lv < L; ++lv)
+            v += bb[p * L + lv] * blim[lv].d[k] + cb[p * L + lv] * bcsd_new[lv].d[k];
+        if (j >= 6 + L) {
+            lam_path(c, a.lam, PF_BCSD)[p * L + (j - 6 - L)] = v;
+        } else if (j >= 6) {
+            lam_path(c, a.lam, PF_BOUT)[p * L + (j - 6)] = v;
         } else {
-            q[3] = v;
+            // end state: [wse, protected-WSE part on the WSE, protected depth, total storage]
+            const int end = j & 1;
+            double* q = peb(c, a.scr) + 8L * p + 4 * end;
+            if (j < 2) {
+                q[0] = v;
+            } else if (j < 4) {
+                const int e = end ? di : ci;
+                bool to_pdep = false;
+                if (c.lev && (c.flags[e] & CMF_CELL_LEVEE)) {
+                    const double wse = X[F_RDEP * N + e] + (c.celv[e] - c.rh[e]);
+                    to_pdep = c.celv[e] + X[F_PDEP * N + e] <= wse;
+                }
+                q[1] = to_pdep ? 0.0 : v;
+                q[2] = to_pdep ? v : 0.0;
+            } else {
+                q[3] = v;
+            }
         }
     }
 }
@@ -1180,7 +1202,7 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const 
     if ((int)blockIdx.x >= c.grid_cells) {
         // trailing blocks: path direction threads, then dam direction threads
         const long b = (long)blockIdx.x - c.grid_cells;
-        const long pb = c.bif ? (c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock : 0;
+        const long pb = c.bif ? (c.P * path_threads(c.L) + kBlock - 1) / kBlock : 0;
         if (b < pb) path_reverse(c, X, dt, a, b * blockDim.x + threadIdx.x);
         else dam_reverse(c, X, runoff, dt, a, (b - pb) * blockDim.x + threadIdx.x);
         return;
@@ -1628,7 +1650,7 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         if (c.bif) launch_dep(kr_stage_path, c.grid_paths, s, c, X, a);
         launch_dep(kr_limit, c.grid_cells, s, c, X, dt, a);
         // cells, then the path and dam direction threads in trailing blocks
-        const int path_blocks = c.bif ? (int)((c.P * (6 + 2 * c.L) + kBlock - 1) / kBlock) : 0;
+        const int path_blocks = c.bif ? (int)((c.P * path_threads(c.L) + kBlock - 1) / kBlock) : 0;
         const int dam_blocks = (c.res && c.ND > 0) ? (int)((c.ND * kDamDirs + kBlock - 1) / kBlock) : 0;
         launch_dep(kr_momentum, c.grid_cells + path_blocks + dam_blocks, s, c, X, runoff, dt, a);
     }

@@ -7,7 +7,8 @@
 //                    arithmetic, CUDA's fmax/fmin/sqrt/cbrt/exp/log;
 //   double, Dual     the adjoint (cmf_adjoint.cu): its primal on double and
 //                    its Jacobian columns on Dual, a forward-mode dual number
-//                    (value and one directional derivative).
+//                    (value and one directional derivative), or on DualN<K>
+//                    (value and K directional derivatives in one pass).
 //
 // Conventions of the Dual operations (those of the PyTorch transcription the
 // adjoint is checked against, for the branches evaluated this way): smax and
@@ -113,6 +114,143 @@ __device__ __forceinline__ Dual xsub(Dual a, Dual b) { return a - b; }
 __device__ __forceinline__ float xdiv(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ Dual xdiv(Dual a, Dual b) { return a / b; }
+
+// ---------------------------------------------------------------------------
+// DualN<K>: a value and K directional derivatives, carried through one
+// evaluation.  A Jacobian-vector product over K input directions then costs
+// one pass whose primal part (the divisions, roots and branches) runs once
+// instead of K times.  Same conventions as Dual; quotients scale the
+// derivatives by one reciprocal of the divisor.
+// ---------------------------------------------------------------------------
+template <int K>
+struct DualN {
+    double v;
+    double d[K];
+    DualN() = default;
+    __host__ __device__ constexpr DualN(double value) : v(value), d{} {}
+};
+
+template <int K>
+__device__ __forceinline__ DualN<K> scaled(const DualN<K>& a, double value, double f)
+{
+    DualN<K> r;
+    r.v = value;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * f;
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ DualN<K> operator+(const DualN<K>& a, const DualN<K>& b)
+{
+    DualN<K> r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator-(const DualN<K>& a, const DualN<K>& b)
+{
+    DualN<K> r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator-(const DualN<K>& a) { return scaled(a, -a.v, -1.0); }
+template <int K>
+__device__ __forceinline__ DualN<K> operator*(const DualN<K>& a, const DualN<K>& b)
+{
+    DualN<K> r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator/(const DualN<K>& a, const DualN<K>& b)
+{
+    DualN<K> r;
+    r.v = a.v / b.v;
+    const double inv = 1.0 / b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * inv;
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator+(const DualN<K>& a, double b)
+{
+    DualN<K> r = a;
+    r.v = a.v + b;
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator+(double a, const DualN<K>& b) { return b + a; }
+template <int K>
+__device__ __forceinline__ DualN<K> operator-(const DualN<K>& a, double b)
+{
+    DualN<K> r = a;
+    r.v = a.v - b;
+    return r;
+}
+template <int K>
+__device__ __forceinline__ DualN<K> operator-(double a, const DualN<K>& b) { return scaled(b, a - b.v, -1.0); }
+template <int K>
+__device__ __forceinline__ DualN<K> operator*(const DualN<K>& a, double b) { return scaled(a, a.v * b, b); }
+template <int K>
+__device__ __forceinline__ DualN<K> operator*(double a, const DualN<K>& b) { return scaled(b, a * b.v, a); }
+template <int K>
+__device__ __forceinline__ DualN<K> operator/(const DualN<K>& a, double b) { return scaled(a, a.v / b, 1.0 / b); }
+template <int K>
+__device__ __forceinline__ DualN<K> operator/(double a, const DualN<K>& b)
+{
+    const double q = a / b.v;
+    return scaled(b, q, -q / b.v);
+}
+
+template <int K>
+__device__ __forceinline__ double val(const DualN<K>& x) { return x.v; }
+template <int K>
+__device__ __forceinline__ DualN<K> smax(const DualN<K>& a, const DualN<K>& b) { return a.v >= b.v ? a : b; }
+template <int K>
+__device__ __forceinline__ DualN<K> smin(const DualN<K>& a, const DualN<K>& b) { return a.v <= b.v ? a : b; }
+template <int K>
+__device__ __forceinline__ DualN<K> ssqrt(const DualN<K>& a)
+{
+    const double s = sqrt(a.v);
+    return scaled(a, s, a.v > 0.0 ? 0.5 / s : 0.0);
+}
+template <int K>
+__device__ __forceinline__ DualN<K> scbrt(const DualN<K>& a)
+{
+    const double c = cbrt(a.v);
+    return scaled(a, c, a.v != 0.0 ? 1.0 / (3.0 * c * c) : 0.0);
+}
+template <int K>
+__device__ __forceinline__ DualN<K> sexp(const DualN<K>& a)
+{
+    const double e = exp(a.v);
+    return scaled(a, e, e);
+}
+template <int K>
+__device__ __forceinline__ DualN<K> slog(const DualN<K>& a) { return scaled(a, log(a.v), 1.0 / a.v); }
+template <int K>
+__device__ __forceinline__ DualN<K> sabs(const DualN<K>& a)
+{
+    return scaled(a, fabs(a.v), (double)((a.v > 0.0) - (a.v < 0.0)));
+}
+template <int K>
+__device__ __forceinline__ DualN<K> xfma(const DualN<K>& a, const DualN<K>& b, const DualN<K>& c) { return a * b + c; }
+template <int K>
+__device__ __forceinline__ DualN<K> xmul(const DualN<K>& a, const DualN<K>& b) { return a * b; }
+template <int K>
+__device__ __forceinline__ DualN<K> xadd(const DualN<K>& a, const DualN<K>& b) { return a + b; }
+template <int K>
+__device__ __forceinline__ DualN<K> xsub(const DualN<K>& a, const DualN<K>& b) { return a - b; }
+template <int K>
+__device__ __forceinline__ DualN<K> xdiv(const DualN<K>& a, const DualN<K>& b) { return a / b; }
 
 // positive part, written as the comparison the storage clips use (a NaN or a
 // negative zero becomes +0)
