@@ -1121,8 +1121,8 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
 // kr_stage_path, and writes only the path lambdas and the path-end buffer,
 // none of which the momentum or dam reverse touches.  Two lanes: wider
 // numbers spill under the launch's 64-register cap (measured on the 250k
-// full-physics window: 247 us per reverse sub-step at 2 lanes, 253 at 4,
-// 293 at 8, 265 with one direction per thread).
+// full-physics window, forward plus adjoint per sub-step: 247 us at 2 lanes,
+// 253 at 4, 293 at 8, 265 with one direction per thread).
 #ifndef CMF_ADJ_PATH_LANES
 #define CMF_ADJ_PATH_LANES 2
 #endif
