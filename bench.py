@@ -474,6 +474,93 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
                         "state reset copies of the looped runs"}
 
 
+def small_network_measure(device, name: str, days: int) -> dict:
+    """One of the small benchmark configurations (plain_60k: 60,000
+    catchments, plain physics, daily runoff, the 3600 s dt cap; full_250k:
+    250,000 catchments with full physics) routed through the public API over
+    `days` daily intervals after one warm-up day, three ways on the same GPU:
+    the interval graph, the persistent interval kernel, and the reference's
+    own CUDA kernels (oracle/_ref, driven as CaMaFlood.step_advance drives
+    them).  A sub-step here is a few microseconds of work, so launch and
+    barrier costs decide.  The three end states are compared field by field.
+    The reference has no dt cap, so on plain_60k its arm runs the capped count
+    max(n, T / 3600 s) as a fixed count, as the parity test does."""
+    import torch
+    from cmfb200 import CaMaFlood, synthetic as syn
+    from oracle import oracle as O, ref_cuda as RC
+    cfg = syn.CONFIGS[name]
+    net = syn.generate(cfg["spec"])
+    cap_s = cfg.get("max_sub_step_seconds", 0.0)
+    T = cfg["interval"]
+    stream = torch.cuda.current_stream(device)
+    out = {"catchments": net.num_catchments, "days": days, "warmup_days": 1,
+           "modules": list(net.opened_modules)}
+    states = {}
+    for mode in ("graph", "persistent"):
+        m = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=net.opened_modules,
+                      step_duration=T, max_sub_step_seconds=cap_s, persistent=(mode == "persistent"))
+        run = [torch.as_tensor(syn.daily_runoff(net, d)[m.order]).to(device) for d in range(days + 1)]
+        m.set_inputs(run[0])
+        m.step_advance()
+        cnt = torch.zeros(days, dtype=torch.int32, device=device)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for d in range(days):
+            m.set_inputs(run[d + 1])
+            m.step_advance()
+            cnt[d].copy_(m.sub_step_counts()[0])
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        m.check_status()
+        subs = int(cnt.sum().item())
+        ms = e0.elapsed_time(e1)
+        out[mode] = {"value": net.num_catchments * subs / (ms / 1e3), "sub_steps": subs,
+                     "us_per_substep": 1e3 * ms / subs}
+        states[mode] = {k: v.cpu().numpy().copy() for k, v in m.state_tensors().items()}
+        order = m.order
+        m.close()
+    out["persistent_over_graph"] = out["persistent"]["value"] / out["graph"]["value"]
+    out["persistent_state_equal"] = all(np.array_equal(states["graph"][k], states["persistent"][k])
+                                        for k in states["graph"])
+    if RC.available():
+        ref = RC.RefCuda(O.reference_fields(net.fields, net.opened_modules), net.opened_modules,
+                         device=device)
+        cap_n = int(round(T / cap_s)) if cap_s > 0 else 0
+        run = [torch.as_tensor(syn.daily_runoff(net, d)).to(device) for d in range(days + 1)]
+
+        def ref_step(d):
+            ref.t["runoff"].copy_(run[d])
+            if cap_n:
+                n = max(ref.adaptive_sub_steps(T), cap_n)
+                return ref.step_advance(T, adaptive=False, fixed_n=n)
+            return ref.step_advance(T)
+
+        ref_step(0)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        subs = 0
+        for d in range(days):
+            subs += ref_step(d + 1)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        out["reference_cuda"] = {"value": net.num_catchments * subs / (ms / 1e3), "sub_steps": subs,
+                                 "us_per_substep": 1e3 * ms / subs}
+        equal = True
+        for k, a in states["graph"].items():
+            b = ref.t[k].detach().cpu().numpy()
+            if a.ndim == 1 and not k.startswith("bifurcation_"):
+                b = b[order]
+            equal = equal and bool(np.array_equal(a, b))
+        out["reference_cuda"]["state_equal"] = equal
+        best = max(out["graph"]["value"], out["persistent"]["value"])
+        out["ours_best_over_reference_cuda"] = best / out["reference_cuda"]["value"]
+        del ref
+    return out
+
+
 def adjoint_compare(device, days: int, checkpoint_every: int = 96, repeats: int = 5) -> dict:
     """Forward+adjoint against forward on the calibration window: the
     250k-catchment full-physics network (8,000 bifurcation paths, levees on
@@ -1053,6 +1140,12 @@ def run_ours(args) -> None:
                                     member_tile=args.ensemble_member_tile,
                                     block=args.ensemble_block, days=args.ensemble_days)
 
+    small = None
+    if world == 1 and args.small_networks:
+        model.close()
+        small = {"plain_60k": small_network_measure(device, "plain_60k", 29),
+                 "full_250k": small_network_measure(device, "full_250k", 10)}
+
     adjoint = None
     if world == 1 and args.adjoint_days > 0:
         model.close()
@@ -1087,6 +1180,7 @@ def run_ours(args) -> None:
             "reference_cuda": ref_cuda,
             "cpu_baseline": cpu,
             "ensemble": ensemble,
+            "small_networks": small,
             "adjoint": adjoint,
             "forcing": forcing_leg,
             "statistics": stats,
@@ -1173,6 +1267,9 @@ def main() -> None:
                     help="simulated days routed before the timed intervals (a warm, flooded state)")
     ap.add_argument("--no-reference-cuda", dest="reference_cuda", action="store_false",
                     help="skip timing the reference's own CUDA kernels on the same workload")
+    ap.add_argument("--no-small-networks", dest="small_networks", action="store_false",
+                    help="skip the small-configuration leg (60k plain and 250k full physics: "
+                         "interval graph, persistent kernel and the reference's CUDA kernels)")
     ap.add_argument("--probe-kernels", action="store_true",
                     help="launch each sub-step kernel once on the spun-up workload inside an "
                          "NVTX range 'probe' (for a profiler) and exit")

@@ -25,6 +25,7 @@ CMF_ERR_UNSUPPORTED = 5
 
 STATUS_NONFINITE = 1
 STATUS_SUBSTEP_CAP = 2
+STATUS_SYNC_TIMEOUT = 8
 
 FEAT_BIFURCATION = 1
 FEAT_LEVEE = 2
@@ -169,6 +170,8 @@ def lib() -> ctypes.CDLL:
     h.cmf_plan_destroy.argtypes = [_P]
     h.cmf_plan_set_member_tile.restype = ctypes.c_int
     h.cmf_plan_set_member_tile.argtypes = [_P, _I32]
+    h.cmf_plan_set_persistent.restype = ctypes.c_int
+    h.cmf_plan_set_persistent.argtypes = [_P, ctypes.c_int]
     h.cmf_step_interval.restype = ctypes.c_int
     h.cmf_step_interval.argtypes = [_P, _P, _F64, _I32]
     h.cmf_phase_momentum.restype = ctypes.c_int

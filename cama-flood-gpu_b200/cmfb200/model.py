@@ -149,7 +149,8 @@ class CaMaFlood:
                  max_sub_step_seconds: float = 0.0, max_sub_steps_cap: int = 0,
                  gravity: float = 9.8, min_kinematic_slope: float = 1.0e-5,
                  adaptive_time_factor: float = 0.7, budget: bool = False,
-                 variables_to_save: Optional[Mapping[str, Iterable[str]]] = None):
+                 variables_to_save: Optional[Mapping[str, Iterable[str]]] = None,
+                 persistent: bool = False):
         if input_proxy is None:
             raise ValueError("input_proxy (field name -> array mapping) is required")
         mods = set(opened_modules) | {"base"}
@@ -177,12 +178,15 @@ class CaMaFlood:
         self.max_sub_steps_cap = int(max_sub_steps_cap)
         self.budget_enabled = bool(budget) or "log" in mods
         self.member_tile = 1
+        self.persistent = False
         self._plan = None
         self._prepare(dict(input_proxy), dict(batched_fields or {}))
         self._upload()
         self._init_statistics(variables_to_save or {})
         self._create_plan()
         self.reset_statistics()
+        if persistent:
+            self.set_persistent(True)
 
     # ------------------------------------------------------------------ #
     # construction
@@ -559,6 +563,8 @@ class CaMaFlood:
         if self.member_tile != 1:
             _lib.check(lib.cmf_plan_set_member_tile(plan, self.member_tile), "plan_set_member_tile")
         self._attach_statistics()
+        if self.persistent:
+            _lib.check(lib.cmf_plan_set_persistent(plan, 1), "plan_set_persistent")
 
     # ------------------------------------------------------------------ #
     # output statistics (variables_to_save)
@@ -783,6 +789,19 @@ class CaMaFlood:
         _lib.check(_lib.lib().cmf_plan_set_member_tile(self._plan, width), "plan_set_member_tile")
         self.member_tile = width
 
+    def set_persistent(self, on: bool = True) -> None:
+        """Run each interval's sub-steps in one persistent cooperative kernel
+        (grid-wide barriers between the phases) instead of the interval
+        graph; the results are the same.  It pays on small networks, where a
+        sub-step is a few microseconds of work.  One member, no budget and no
+        output statistics; raises otherwise."""
+        rc = _lib.lib().cmf_plan_set_persistent(self._plan, 1 if on else 0)
+        if rc == _lib.CMF_ERR_UNSUPPORTED:
+            raise ValueError("the persistent interval kernel runs one member without budget or "
+                             "output statistics")
+        _lib.check(rc, "plan_set_persistent")
+        self.persistent = bool(on)
+
     def autotune_block_size(self, candidates=None, sub_steps: int = 6,
                             cache_path: Optional[str] = None, tile_candidates=None) -> dict:
         """Measure the candidate CTA sizes (and, with several members, member
@@ -807,6 +826,8 @@ class CaMaFlood:
             raise FloatingPointError("routing produced non-finite storage or discharge")
         if s & _lib.STATUS_SUBSTEP_CAP:
             raise RuntimeError("CFL asked for more sub-steps than max_sub_steps_cap")
+        if s & _lib.STATUS_SYNC_TIMEOUT:
+            raise RuntimeError("a grid barrier of the persistent interval kernel timed out")
 
     # ------------------------------------------------------------------ #
     # ordering helpers, state I/O

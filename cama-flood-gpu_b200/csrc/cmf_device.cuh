@@ -43,6 +43,11 @@
 
 // minimum resident 256-thread CTAs per SM (register caps) of the sub-step kernels;
 // k_stage: 4 (64 registers, no spills)
+// minimum resident 256-thread CTAs per SM of the persistent interval kernel
+// (64 registers, the budget of k_stage, which it inlines)
+#ifndef CMF_PERSIST_MIN_BLOCKS
+#define CMF_PERSIST_MIN_BLOCKS 4
+#endif
 #ifndef CMF_STAGE_MIN_BLOCKS
 #define CMF_STAGE_MIN_BLOCKS 4
 #endif
@@ -73,6 +78,8 @@ constexpr int kBudgetTerms = CMF_BUDGET_TERMS;
 constexpr int kCtlStep = 0;       // current sub-step index k
 constexpr int kCtlMaxSteps = 1;   // max over members of the sub-step count
 constexpr int kCtlBlocksDone = 2; // last-block-done counter of k_stage
+constexpr int kCtlBarrier = 4;    // [4..5]: arrival counter (u64) of the persistent kernel's grid barrier
+constexpr int kCtlAbort = 6;      // set when a grid barrier gave up: every block leaves the interval
 constexpr int kHardSubStepCap = 100000;  // bound of the device-side sub-step loop
 
 // Two fluxes of one element stored together (river, floodplain): one 8-byte
@@ -763,6 +770,17 @@ __device__ __forceinline__ void stage_path(const Dev<REAL>& v, long p, int m, in
 // cell and its bifurcation partners.
 // ---------------------------------------------------------------------------
 template <typename REAL, bool ONE, bool BIF>
+__device__ __forceinline__ void limit_cell(const Dev<REAL>& v, long i, int m, int kh)
+{
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
+    if (!st.active) return;
+    const int k = st.k;
+    const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
+    const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
+    v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
+}
+
+template <typename REAL, bool ONE, bool BIF>
 __global__ void __launch_bounds__(256, (sizeof(REAL) == 4 ? 8 : 4)) k_limit(const Dev<REAL> v, int kh)
 {
     const int W = mtile_of<REAL, ONE>(v);
@@ -772,12 +790,7 @@ __global__ void __launch_bounds__(256, (sizeof(REAL) == 4 ? 8 : 4)) k_limit(cons
         if (t >= v.N * (long)v.M) return;
         int m;
         long i = split_member<ONE>(v, t, m);
-        const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, 2);
-        if (!st.active) continue;
-        const int k = st.k;
-        const double* rsrc = (k & 1) ? v.rs1 : v.rs0;
-        const double* fsrc = (k & 1) ? v.fs1 : v.fs0;
-        v.lrs[ix<ONE>(i, m, v.M)] = limit_rate_of<REAL, ONE, BIF>(v, rsrc, fsrc, i, m, v.dt[m]);
+        limit_cell<REAL, ONE, BIF>(v, i, m, kh);
     }
 }
 
@@ -806,6 +819,63 @@ __device__ __forceinline__ void advance_step(int* ctl, cudaGraphConditionalHandl
 // levee cells are a scattered minority, and running their long scan inside
 // k_stage would stretch every CTA of the much larger catchment grid.
 // ---------------------------------------------------------------------------
+// One levee (list index li) of member m: re-partition of its cell's
+// flood-stage result, as k_levee and the persistent interval kernel run it.
+template <typename REAL, bool ONE>
+__device__ __forceinline__ void levee_cell(const Dev<REAL>& v, long li, int m, int kh, int force_diag)
+{
+    const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
+    if (!st.active) return;
+    const int k = st.k;
+    double* rdst = (k & 1) ? v.rs0 : v.rs1;
+    double* fdst = (k & 1) ? v.fs0 : v.fs1;
+    const long ci = v.lci[li];
+    const long cm = ix<ONE>(ci, m, v.M);
+    LeveeState<double, REAL> lst;
+    lst.rs = rdst[cm];
+    lst.fs = fdst[cm];
+    lst.rdep = v.rdep[cm];
+    lst.fdep = v.fdep[cm];
+    lst.ffr = v.ffr[cm];
+    // static fields from the levee-indexed copies where the plan keeps
+    // them (coalesced over the levee list), else from the cells
+    const REAL* row = v.lpk_tbl ? v.lpk_tbl + li * (long)v.K : v.tbl + ci * (long)v.K;
+    auto depth = [row](int l) { return row[l]; };
+    REAL rh, rw, rl;
+    if (v.lpk_geo) {
+        rh = v.lpk_geo[li];
+        rw = v.lpk_geo[v.NLV + li];
+        rl = v.lpk_geo[2 * v.NLV + li];
+    } else {
+        rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, ci, m, v.M);
+        rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
+        rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
+    }
+    const REAL crown = v.lcrown[li], frac = v.lfrac[li], base = v.lbase[li];
+    if (v.lmk) {
+        // the plan's marks: the row is read only while the protected
+        // side fills
+        const long n = v.NLV;
+        LeveeMarks<REAL, REAL> mk;
+        mk.s_base = v.lmk[li];
+        mk.s_crown = v.lmk[n + li];
+        mk.s_top = v.lmk[2 * n + li];
+        mk.s_first = v.lmk[3 * n + li];
+        mk.dw = v.lmk[4 * n + li];
+        mk.dist = v.lmk[5 * n + li];
+        levee_apply<0>(lst, mk, rw, rh, rl, crown, frac, base, v.K, depth);
+    } else {
+        levee_partition<0>(lst, rw, rh, rl, v.ca[ci], crown, frac, base, v.K, depth);
+    }
+    rdst[cm] = lst.rs;
+    fdst[cm] = lst.fs;
+    v.ps[cm] = lst.ps;
+    v.rdep[cm] = lst.rdep;
+    v.fdep[cm] = lst.fdep;
+    v.pdep[cm] = lst.pdep;
+    v.ffr[cm] = lst.ffr;
+}
+
 template <typename REAL, bool ONE>
 __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int advance)
@@ -817,57 +887,7 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
         if (t >= v.NLV * (long)v.M) break;
         int m;
         const long li = split_member<ONE>(v, t, m);
-        const StepInfo st = step_info<ONE>(v.ctl, v.nsub, kh, m, force_diag);
-        if (st.active) {
-            const int k = st.k;
-            double* rdst = (k & 1) ? v.rs0 : v.rs1;
-            double* fdst = (k & 1) ? v.fs0 : v.fs1;
-            const long ci = v.lci[li];
-            const long cm = ix<ONE>(ci, m, v.M);
-            LeveeState<double, REAL> lst;
-            lst.rs = rdst[cm];
-            lst.fs = fdst[cm];
-            lst.rdep = v.rdep[cm];
-            lst.fdep = v.fdep[cm];
-            lst.ffr = v.ffr[cm];
-            // static fields from the levee-indexed copies where the plan keeps
-            // them (coalesced over the levee list), else from the cells
-            const REAL* row = v.lpk_tbl ? v.lpk_tbl + li * (long)v.K : v.tbl + ci * (long)v.K;
-            auto depth = [row](int l) { return row[l]; };
-            REAL rh, rw, rl;
-            if (v.lpk_geo) {
-                rh = v.lpk_geo[li];
-                rw = v.lpk_geo[v.NLV + li];
-                rl = v.lpk_geo[2 * v.NLV + li];
-            } else {
-                rh = par<ONE>(v.rh, CMF_BATCH_RIVER_HEIGHT, v.batched, ci, m, v.M);
-                rw = par<ONE>(v.rw, CMF_BATCH_RIVER_WIDTH, v.batched, ci, m, v.M);
-                rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
-            }
-            const REAL crown = v.lcrown[li], frac = v.lfrac[li], base = v.lbase[li];
-            if (v.lmk) {
-                // the plan's marks: the row is read only while the protected
-                // side fills
-                const long n = v.NLV;
-                LeveeMarks<REAL, REAL> mk;
-                mk.s_base = v.lmk[li];
-                mk.s_crown = v.lmk[n + li];
-                mk.s_top = v.lmk[2 * n + li];
-                mk.s_first = v.lmk[3 * n + li];
-                mk.dw = v.lmk[4 * n + li];
-                mk.dist = v.lmk[5 * n + li];
-                levee_apply<0>(lst, mk, rw, rh, rl, crown, frac, base, v.K, depth);
-            } else {
-                levee_partition<0>(lst, rw, rh, rl, v.ca[ci], crown, frac, base, v.K, depth);
-            }
-            rdst[cm] = lst.rs;
-            fdst[cm] = lst.fs;
-            v.ps[cm] = lst.ps;
-            v.rdep[cm] = lst.rdep;
-            v.fdep[cm] = lst.fdep;
-            v.pdep[cm] = lst.pdep;
-            v.ffr[cm] = lst.ffr;
-        }
+        levee_cell<REAL, ONE>(v, li, m, kh, force_diag);
     }
     if (kh == -1 && advance) advance_step(v.ctl, h, 1);
 }
@@ -902,6 +922,99 @@ __global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<R
     }
     // With levees, k_levee is the last kernel of the sub-step and advances.
     if (!LEV && kh == -1) advance_step(v.ctl, h, set_cond);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent interval kernel (one member, no budget or statistics): every
+// sub-step of a forcing interval in one cooperative launch.  The blocks walk
+// the catchments, paths and levees in grid-stride loops and meet at a
+// grid-wide barrier after each phase (momentum, limit rate, stage, levee),
+// where the interval graph has a kernel boundary; the per-element work is
+// the same device functions the four sub-step kernels call, with the step
+// index passed explicitly.  On small networks the sub-step is a few
+// microseconds of work, and a barrier costs less than a graph's kernel
+// boundary.
+//
+// The barrier counts arrivals on a monotone 64-bit counter (reset by
+// k_interval_plan): the b-th barrier of the launch completes when the counter
+// reaches (b + 1) x gridDim.x.  All blocks are co-resident (cooperative
+// launch), so every wait ends; each is still bounded in time, after which the
+// block raises CMF_STATUS_SYNC_TIMEOUT and the abort flag, and every block
+// leaves the interval at its next barrier.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kBarrierTimeoutNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long x;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+    return x;
+}
+
+// false: the interval was abandoned (a barrier gave up); the caller returns.
+__device__ __forceinline__ bool grid_barrier(int* ctl, int* status, unsigned long long& target)
+{
+    __shared__ int go_on;
+    __syncthreads();
+    target += gridDim.x;
+    if (threadIdx.x == 0) {
+        unsigned long long* count = reinterpret_cast<unsigned long long*>(ctl + kCtlBarrier);
+        volatile int* abort_flag = ctl + kCtlAbort;
+        __threadfence();
+        atomicAdd(count, 1ull);
+        int ok = 1;
+        const unsigned long long t0 = global_ns();
+        while (load_acquire_u64(count) < target) {
+            if (*abort_flag) { ok = 0; break; }
+            if (global_ns() - t0 > kBarrierTimeoutNs) {
+                atomicOr(status, CMF_STATUS_SYNC_TIMEOUT);
+                atomicExch(ctl + kCtlAbort, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(100);
+        }
+        __threadfence();
+        go_on = ok;
+    }
+    __syncthreads();
+    return go_on != 0;
+}
+
+template <typename REAL, bool RES, bool LEV, bool BIF>
+__global__ void __launch_bounds__(256, CMF_PERSIST_MIN_BLOCKS) k_persistent(const Dev<REAL> v)
+{
+    const int n = v.ctl[kCtlMaxSteps];
+    const long first = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long stride = (long)gridDim.x * blockDim.x;
+    unsigned long long target = 0;
+    double bud[kBudgetTerms];
+    for (int k = 0; k < n; ++k) {
+        for (long i = first; i < v.N; i += stride)
+            momentum_cell<REAL, true, RES, LEV, BIF>(v, i, 0, k, 0);
+        if (BIF)
+            for (long p = first; p < v.P; p += stride) momentum_path<REAL, true, RES, LEV>(v, p, 0, k);
+        if (!grid_barrier(v.ctl, v.status, target)) return;
+        for (long i = first; i < v.N; i += stride) limit_cell<REAL, true, BIF>(v, i, 0, k);
+        if (!grid_barrier(v.ctl, v.status, target)) return;
+        for (long i = first; i < v.N; i += stride)
+            stage_cell<REAL, true, RES, LEV, BIF, false>(v, i, 0, k, 0, bud);
+        if (BIF)
+            for (long p = first; p < v.P; p += stride) stage_path<REAL, true, BIF>(v, p, 0, k);
+        if (!grid_barrier(v.ctl, v.status, target)) return;
+        if (LEV) {
+            for (long l = first; l < v.NLV; l += stride) levee_cell<REAL, true>(v, l, 0, k, 0);
+            if (!grid_barrier(v.ctl, v.status, target)) return;
+        }
+    }
+    if (first == 0) v.ctl[kCtlStep] = n;
 }
 
 // ---------------------------------------------------------------------------
@@ -996,6 +1109,8 @@ __global__ void k_interval_plan(const Dev<REAL> v, int fixed_n, cudaGraphConditi
     if (threadIdx.x == 0) {
         v.ctl[kCtlMaxSteps] = smax;
         v.ctl[kCtlStep] = 0;
+        *reinterpret_cast<unsigned long long*>(v.ctl + kCtlBarrier) = 0ull;
+        v.ctl[kCtlAbort] = 0;
         if (set_cond) cudaGraphSetConditional(h, smax > 0 ? 1u : 0u);
     }
 }

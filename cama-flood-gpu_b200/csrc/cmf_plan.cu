@@ -43,6 +43,7 @@ struct KernelSet {
     const void* stats_acc;
     const void* stats_reset;
     const void* stats_fin;
+    const void* persist;  // persistent interval kernel (one member, no budget), else null
 };
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUD>
@@ -61,6 +62,8 @@ KernelSet make_set()
     k.stats_acc = (const void*)k_stats_accumulate<REAL, ONE>;
     k.stats_reset = (const void*)k_stats_reset<REAL, ONE>;
     k.stats_fin = (const void*)k_stats_finalize<REAL, ONE>;
+    if constexpr (ONE && !BUD) k.persist = (const void*)k_persistent<REAL, RES, LEV, BIF>;
+    else k.persist = nullptr;
     return k;
 }
 
@@ -162,6 +165,9 @@ struct CmfPlan {
     int graph_fixed;
     // output statistics folded in after every sub-step (count == 0: none)
     StatsArgs stats;
+    // persistent interval kernel instead of the interval graph
+    bool persistent;
+    int persist_grid;
 };
 
 namespace {
@@ -531,6 +537,41 @@ int interval_direct(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
     return CMF_OK;
 }
 
+// One interval through the persistent kernel: the prologue kernels, then
+// every sub-step in one cooperative launch, then the epilogue.
+int interval_persistent(CmfPlan* p, cudaStream_t s, double T, int fixed_n)
+{
+    const CmfView& v = p->view;
+    int rc;
+    const int adaptive = fixed_n <= 0 ? 1 : 0;
+    {
+        int a = adaptive;
+        void* args[] = {p->dev, &T, &a};
+        if ((rc = launch(p->ks.begin, 1, 32, args, s)) != CMF_OK) return rc;
+    }
+    if (adaptive) {
+        void* args[] = {p->dev};
+        const int cfl_blocks = ceil_div((long)v.num_catchments * v.num_members, p->tpb);
+        if ((rc = launch(p->ks.cfl, cfl_blocks, p->tpb, args, s)) != CMF_OK) return rc;
+    }
+    {
+        int f = fixed_n;
+        cudaGraphConditionalHandle h = 0;
+        int set = 0;
+        void* args[] = {p->dev, &f, &h, &set};
+        if ((rc = launch(p->ks.plan, 1, 256, args, s)) != CMF_OK) return rc;
+    }
+    {
+        void* args[] = {p->dev};
+        if ((rc = check_cuda(cudaLaunchCooperativeKernel(p->ks.persist, dim3(p->persist_grid),
+                                                          dim3(p->tpb), args, 0, s))) != CMF_OK)
+            return rc;
+    }
+    void* args[] = {p->dev};
+    const int eb = ceil_div((long)v.num_catchments * v.num_members, 256);
+    return launch(p->ks.end, eb, 256, args, s);
+}
+
 }  // namespace
 
 extern "C" {
@@ -671,6 +712,7 @@ int cmf_step_interval(CmfPlan* p, void* stream, double outer_seconds, int32_t fi
     int fixed = p->adaptive ? (fixed_sub_steps > 0 ? fixed_sub_steps : 0)
                             : (fixed_sub_steps > 0 ? fixed_sub_steps : -1);
     if (fixed < 0) return CMF_ERR_ARG;  // fixed mode needs a sub-step count
+    if (p->persistent) return interval_persistent(p, s, outer_seconds, fixed);
     if (!p->graph_enabled) return interval_direct(p, s, outer_seconds, fixed);
     int rc;
     const bool adaptive_now = fixed == 0;
@@ -834,6 +876,34 @@ int cmf_budget_flush(CmfPlan* p, void* stream)
     return launch((const void*)k_budget_flush, 1, 256, args, (cudaStream_t)stream);
 }
 
+int cmf_plan_set_persistent(CmfPlan* p, int enable)
+{
+    if (!p) return CMF_ERR_ARG;
+    if (!enable) {
+        p->persistent = false;
+        return CMF_OK;
+    }
+    if (!p->ks.persist || p->stats.count > 0) return CMF_ERR_UNSUPPORTED;
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    int rc;
+    if ((rc = check_cuda(cudaGetDevice(&dev))) != CMF_OK) return rc;
+    if ((rc = check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev))) != CMF_OK) return rc;
+    if ((rc = check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) != CMF_OK) return rc;
+    if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, p->ks.persist, p->tpb, 0)))
+        != CMF_OK)
+        return rc;
+    if (!coop || per_sm < 1) return CMF_ERR_UNSUPPORTED;
+    const CmfView& v = p->view;
+    long work = v.num_catchments;
+    if (p->path_blocks > 0 && v.num_bifurcation_paths > work) work = v.num_bifurcation_paths;
+    if (p->levee_blocks > 0 && v.num_levees > work) work = v.num_levees;
+    const int need = ceil_div(work, p->tpb);
+    const int resident = per_sm * sms;
+    p->persist_grid = need < resident ? (need > 0 ? need : 1) : resident;
+    p->persistent = true;
+    return CMF_OK;
+}
+
 int cmf_plan_set_member_tile(CmfPlan* p, int32_t width)
 {
     if (!p || width < 1) return CMF_ERR_ARG;
@@ -862,6 +932,7 @@ int cmf_stats_attach(CmfPlan* p, int count, const CmfStatistic* stats, double* w
 {
     if (!p || count < 0 || count > CMF_MAX_STATISTICS) return CMF_ERR_ARG;
     if (count > 0 && !stats) return CMF_ERR_ARG;
+    if (count > 0 && p->persistent) return CMF_ERR_UNSUPPORTED;  // the persistent kernel folds none in
     StatsArgs a;
     std::memset(&a, 0, sizeof(a));
     const bool lev = p->view.features & CMF_FEAT_LEVEE;

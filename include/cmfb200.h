@@ -44,6 +44,7 @@ extern "C" {
 /* ---- device status word bits (CmfView.status[0]) ------------------------- */
 #define CMF_STATUS_NONFINITE 1   /* NaN/Inf storage or discharge produced     */
 #define CMF_STATUS_SUBSTEP_CAP 2 /* CFL asked for more sub-steps than allowed */
+#define CMF_STATUS_SYNC_TIMEOUT 8 /* a grid barrier of the persistent interval kernel gave up */
 
 /* ---- feature bits (CmfView.features) ------------------------------------- */
 #define CMF_FEAT_BIFURCATION 1 /* bifurcation module open                    */
@@ -223,6 +224,18 @@ int cmf_workspace_size(const CmfView* view, size_t* bytes);
  * creates a new plan. */
 int cmf_plan_create(const CmfView* view, CmfPlan** plan);
 void cmf_plan_destroy(CmfPlan* plan);
+/* Persistent interval kernel (no counterpart in the reference; it replaces
+ * the per-sub-step launch loop of cmfgpu/models/cama_flood_model.py:134-162
+ * for small networks).  enable != 0: cmf_step_interval runs every sub-step of
+ * an interval in one cooperative launch whose blocks meet at a grid-wide
+ * barrier after each phase, instead of the interval graph.  Results are the
+ * same.  One member only, no budget and no output statistics
+ * (CMF_ERR_UNSUPPORTED otherwise, and cmf_stats_attach refuses while it is
+ * on); the grid is the device's resident CTAs, or fewer when the network
+ * needs fewer.  A barrier wait that outlasts 1 s raises
+ * CMF_STATUS_SYNC_TIMEOUT and ends the interval.  enable == 0 returns to the
+ * interval graph. */
+int cmf_plan_set_persistent(CmfPlan* plan, int enable);
 /* Member-tile width of the member-batched kernels (no counterpart in the
  * reference): each thread handles `width` consecutive members of one
  * catchment, so the catchment's shared fields are loaded once from HBM and
