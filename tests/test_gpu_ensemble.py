@@ -10,26 +10,35 @@ from cmfb200 import CaMaFlood, synthetic as syn
 pytestmark = pytest.mark.gpu
 
 
-def _plain(net, manning, device):
+def _plain(net, manning, device, precision="float32"):
     f = dict(net.fields)
     f["river_manning"] = manning
-    return CaMaFlood(device=device, input_proxy=f, opened_modules=["base", "adaptive_time"])
+    return CaMaFlood(device=device, input_proxy=f, opened_modules=["base", "adaptive_time"],
+                     precision=precision)
 
 
-@pytest.mark.parametrize("members", [4, 3])
-def test_batched_members_equal_plain_runs(members, device):
+# member counts that are and are not powers of two, with and without a member
+# tile, in fp32 and fp64
+@pytest.mark.parametrize("members,precision", [(4, "float32"), (3, "float32"), (8, "float32"),
+                                               (16, "float32"), (8, "float64")])
+def test_batched_members_equal_plain_runs(members, precision, device):
     net = syn.generate_basins(40, 30_000, seed=9)
     n = net.num_catchments
     rfac, mfac = syn.ensemble_factors(n, members, seed=9)
-    manning = (net.fields["river_manning"][:, None] * mfac).astype(np.float32)
+    real = np.float32 if precision == "float32" else np.float64
+    manning = (net.fields["river_manning"][:, None] * mfac).astype(real)
     ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=["base", "adaptive_time"],
-                    num_members=members, batched_fields={"river_manning": manning})
-    plains = [_plain(net, np.ascontiguousarray(manning[:, m]), device) for m in range(members)]
+                    num_members=members, batched_fields={"river_manning": manning},
+                    precision=precision)
+    if members % 4 == 0 and members > 4:
+        ens.set_member_tile(4)
+    plains = [_plain(net, np.ascontiguousarray(manning[:, m]), device, precision)
+              for m in range(members)]
     order = ens.order
     counts = []
     for day in range(2):
         r = syn.daily_runoff(net, day)
-        rm = (r[:, None] * rfac).astype(np.float32)
+        rm = (r[:, None] * rfac).astype(real)
         ens.set_inputs(torch.as_tensor(rm[order]).to(device))
         ens.step_advance()
         counts.append(ens.sub_step_counts().cpu().numpy().copy())
