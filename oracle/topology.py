@@ -22,8 +22,10 @@ def _fn(name):
     return f
 
 
-def _p(a: np.ndarray) -> int:
-    return a.ctypes.data
+def _p(a: np.ndarray) -> ctypes.c_void_p:
+    # a typed pointer: a bare int would pass as a 32-bit C int and truncate
+    # the addresses of large (mmap-allocated) arrays
+    return ctypes.c_void_p(a.ctypes.data)
 
 
 def accumulate_upstream(downstream_idx, values) -> np.ndarray:
