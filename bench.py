@@ -568,7 +568,7 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96, repeats: int 
     intervals, discharge at 500 cells with upstream area > 1000 km^2,
     relative-misfit loss against a run with river Manning x lognormal(0.2).
     Both are timed with CUDA events on the same GPU from the same spun-up
-    state: one discarded warm-up pair, then `repeats` interleaved repetitions,
+    state: three discarded warm-up pairs, then `repeats` interleaved repetitions,
     medians; the gradient run includes its checkpointed forward."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn, topology
@@ -606,7 +606,7 @@ def adjoint_compare(device, days: int, checkpoint_every: int = 96, repeats: int 
         return torch.autograd.grad(loss, [p["river_manning"], p["river_height"],
                                           p["river_width"], f])
 
-    for _ in range(2):                        # warm-up (allocations, lazy init, clocks)
+    for _ in range(3):                        # warm-up (allocations, lazy init, clocks)
         fwd()
         fwd_adj()
     torch.cuda.synchronize(device)
