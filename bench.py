@@ -1194,6 +1194,52 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def probe_ensemble(args) -> None:
+    """The member-batched form of probe_kernels: the ensemble workload
+    (`--ensemble-members` members of `--ensemble-catchments` catchments in 500
+    basins, runoff and river Manning perturbed per member, member tile
+    `--ensemble-member-tile`, `--ensemble-block`-thread CTAs) routed for
+    `--spinup-days` daily intervals, then each sub-step kernel launched once
+    inside the NVTX range "probe"."""
+    import torch
+    from cmfb200 import CaMaFlood, synthetic as syn, _lib
+    device = torch.device("cuda", 0)
+    members = args.ensemble_members
+    net = syn.generate_basins(500, args.ensemble_catchments, seed=3)
+    rfac, mfac = syn.ensemble_factors(net.num_catchments, members, seed=3)
+    manning = (net.fields["river_manning"][:, None] * mfac).astype(np.float32)
+    ens = CaMaFlood(device=device, input_proxy=net.fields, opened_modules=["base", "adaptive_time"],
+                    num_members=members, batched_fields={"river_manning": manning},
+                    BLOCK_SIZE=args.ensemble_block)
+    ens.set_member_tile(max(1, args.ensemble_member_tile))
+    order = ens.order
+    rf = torch.as_tensor(rfac[order]).to(device)
+
+    def runoff(d):
+        return (torch.as_tensor(syn.daily_runoff(net, d)[order]).to(device)[:, None] * rf).contiguous()
+
+    for d in range(args.spinup_days):
+        ens.set_inputs(runoff(d))
+        ens.step_advance()
+    ens.set_inputs(runoff(args.spinup_days))
+    ens.compute_adaptive_time_step()
+    torch.cuda.synchronize(device)
+    parts = [("k_momentum", _lib.PART_MOMENTUM), ("k_limit", _lib.PART_LIMIT),
+             ("k_stage", _lib.PART_STAGE)]
+    torch.cuda.nvtx.range_push("probe")
+    for _, part in parts:
+        ens.launch_substep_kernel(0, part)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize(device)
+    ens.check_status()
+    print(json.dumps({"probe": [p for p, _ in parts], "members": members,
+                      "catchments": net.num_catchments, "spinup_days": args.spinup_days,
+                      "member_tile": ens.member_tile, "block": ens.block_size,
+                      "flooded_fraction": float((ens.base.flood_storage > 0).double().mean().item())}),
+          flush=True)
+    ens.close()
+
+
 def probe_kernels(args) -> None:
     """One launch of each sub-step kernel on the spun-up workload, outside the
     interval graph and inside an NVTX range named "probe", for a profiler to
@@ -1270,6 +1316,9 @@ def main() -> None:
     ap.add_argument("--no-small-networks", dest="small_networks", action="store_false",
                     help="skip the small-configuration leg (60k plain and 250k full physics: "
                          "interval graph, persistent kernel and the reference's CUDA kernels)")
+    ap.add_argument("--probe-ensemble", action="store_true",
+                    help="with --probe-kernels: probe the member-batched kernels of the ensemble "
+                         "workload instead")
     ap.add_argument("--probe-kernels", action="store_true",
                     help="launch each sub-step kernel once on the spun-up workload inside an "
                          "NVTX range 'probe' (for a profiler) and exit")
@@ -1278,7 +1327,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.probe_kernels:
+    if args.probe_kernels and args.probe_ensemble:
+        probe_ensemble(args)
+    elif args.probe_kernels:
         probe_kernels(args)
     elif args.impl == "reference":
         run_reference(args)
