@@ -471,13 +471,16 @@ class CaMaFlood:
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
 
     def _features(self) -> int:
+        # an opened module with nothing in it (a basin shard without paths,
+        # levees or reservoirs) keeps its module object but runs no kernel
+        # part: the plan is built without its feature
         has = self.has
         f = 0
-        if has.bif:
+        if has.bif and self.bifurcation.num_bifurcation_paths > 0:
             f |= _lib.FEAT_BIFURCATION
-        if has.lev:
+        if has.lev and self.levee.num_levees > 0:
             f |= _lib.FEAT_LEVEE
-        if has.res:
+        if has.res and self.reservoir.num_reservoirs > 0:
             f |= _lib.FEAT_RESERVOIR
         if has.adaptive:
             f |= _lib.FEAT_ADAPTIVE
@@ -578,8 +581,8 @@ class CaMaFlood:
                 if name not in _lib.STAT_VARIABLES:
                     raise ValueError(f"variable '{name}' cannot be saved "
                                      f"(one of {sorted(_lib.STAT_VARIABLES)})")
-                if name.startswith("protected") and not self.has.lev:
-                    raise ValueError(f"'{name}' needs the levee module")
+                if name.startswith("protected") and not (self.has.lev and self.levee.num_levees > 0):
+                    raise ValueError(f"'{name}' needs the levee module with at least one levee")
                 if (name, op) not in items:
                     items.append((name, op))
         if len(items) > _lib.MAX_STATISTICS:
