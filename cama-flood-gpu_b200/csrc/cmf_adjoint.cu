@@ -1110,7 +1110,9 @@ __global__ void __launch_bounds__(kBlock) kr_limit(const Ctx c, const double* X,
     a.scr[S_QFB * N + j] = qf_bar;
 }
 
-// Path momentum reversed (kr_path): each thread takes kPathLanes of the
+// Path momentum reversed on dual numbers (the form built with
+// CMF_ADJ_PATH_HAND=0, kept as the cross-check of path_reverse_hand): each
+// thread takes kPathLanes of the
 // path's input directions (6 end-state inputs and two per level) and
 // evaluates the path flux once on DualN<kPathLanes> numbers seeded with
 // them, so the primal part of the evaluation (roots, divisions, branches)
@@ -1190,6 +1192,206 @@ __device__ __forceinline__ void path_reverse(const Ctx& c, const double* X, doub
     }
 }
 
+// Path momentum reversed by hand (kr_path, one thread per path): the path
+// flux of path_flux evaluated once on doubles with the quantities its
+// reverse needs, then swept backwards.  It gives every input's adjoint in one
+// pass, where the dual-number form needs one evaluation per kPathLanes
+// directions.  Every branch is taken on the primal values exactly as the
+// dual evaluation takes it, with the same subgradients: smax/smin pass the
+// derivative of the first operand on a tie, square roots have derivative 0
+// at 0, |x| has derivative sign(x), and a level whose semi-implicit depth is
+// at most 1e-5 carries a constant zero flux.
+#ifndef CMF_ADJ_PATH_HAND
+#define CMF_ADJ_PATH_HAND 1
+#endif
+
+__device__ __forceinline__ void path_reverse_hand(const Ctx& c, const double* X, double dt,
+                                                  const Adj& a, long p)
+{
+    if (p >= c.P) return;
+    const int L = c.L;
+    const long N = c.N;
+    const int ci = c.bci[p], di = c.bdi[p];
+    double in[6 + 2 * kMaxLevels];
+    path_inputs(c, X, p, in);
+    const double eta_a = in[0], eta_b = in[1], peta_a = in[2], peta_b = in[3];
+    const double st_a = in[4], st_b = in[5];
+    const double len = c.blen[p];
+    const double gdt = c.g * dt;
+    const double cap = 0.005;
+
+    // forward, keeping what the reverse needs
+    const bool top_a = eta_a >= eta_b;
+    const double top = top_a ? eta_a : eta_b;
+    const bool ptop_a = peta_a >= peta_b;
+    const double ptop = c.lev ? (ptop_a ? peta_a : peta_b) : top;
+    const double raw = (eta_a - eta_b) / len;
+    const double t1 = raw >= -cap ? raw : -cap;
+    const double slope = t1 <= cap ? t1 : cap;
+    const bool slope_free = raw >= -cap && t1 <= cap;
+    double q[kMaxLevels], h[kMaxLevels], hs[kMaxLevels];
+    bool live[kMaxLevels], hpos[kMaxLevels];
+    double sum = 0.0;
+    for (int l = 0; l < L; ++l) {
+        const double surface = (c.lev && l > 0) ? ptop : top;
+        const double hraw = surface - c.belv[p * L + l];
+        hpos[l] = hraw >= 0.0;
+        h[l] = hpos[l] ? hraw : 0.0;
+        double h_si;
+        if (c.lev) {
+            h_si = h[l];
+            if (l == 0) {
+                const double r = sqrt(h[l] * in[6 + L]);
+                if (r > 0.0) h_si = r;
+            }
+        } else {
+            const double r1 = sqrt(h[l] * in[6 + L + l]), r2 = sqrt(h[l] * 0.01);
+            h_si = r1 >= r2 ? r1 : r2;
+        }
+        hs[l] = h_si;
+        live[l] = h_si > 1e-5;
+        q[l] = 0.0;
+        if (live[l]) {
+            const double B = c.bwid[p * L + l], n = c.bman[p * L + l];
+            const double qq = in[6 + l] / B;
+            const double drive = qq + gdt * h_si * slope;
+            const double drag = 1.0 + gdt * (n * n) * fabs(qq) * (1.0 / (h_si * h_si * cbrt(h_si)));
+            q[l] = B * drive / drag;
+        }
+        sum = sum + q[l];
+    }
+    const double moved = fabs(sum) * dt;
+    const bool limited = moved > 0.0;
+    const bool st_first = st_a <= st_b;
+    const double smin_st = st_first ? st_a : st_b;
+    double r0 = 1.0, rate = 1.0;
+    if (limited) {
+        r0 = 0.05 * smin_st / moved;
+        rate = r0 <= 1.0 ? r0 : 1.0;
+    }
+
+    // output adjoints: the limited sum (through the end cells' outgoing
+    // storage), each limited level flux and each new depth
+    const double bsum_tape = bsum_of(c, X)[p];
+    double g_sum = 0.0;
+    if (bsum_tape >= 0.0) g_sum += a.scr[S_OGB * N + ci] * dt;
+    if (bsum_tape <= 0.0) g_sum -= a.scr[S_OGB * N + di] * dt;
+    const double* bb = blimb(c, a.scr);
+    const double* cb = bcsdb(c, a.scr);
+
+    // rate and sum
+    double rate_bar = g_sum * sum;
+    for (int l = 0; l < L; ++l) rate_bar += bb[p * L + l] * q[l];
+    double sum_bar = g_sum * rate;
+    double st_a_bar = 0.0, st_b_bar = 0.0;
+    if (limited && r0 <= 1.0) {
+        const double smin_bar = rate_bar * 0.05 / moved;
+        const double moved_bar = -rate_bar * r0 / moved;
+        if (st_first) st_a_bar += smin_bar;
+        else st_b_bar += smin_bar;
+        sum_bar += moved_bar * dt * (double)((sum > 0.0) - (sum < 0.0));
+    }
+
+    // levels
+    double top_bar = 0.0, ptop_bar = 0.0, slope_bar = 0.0;
+    double flux_bar[kMaxLevels], depth_bar[kMaxLevels];
+    for (int l = 0; l < L; ++l) {
+        flux_bar[l] = 0.0;
+        depth_bar[l] = 0.0;
+        double h_bar = cb[p * L + l];
+        if (live[l]) {
+            const double q_bar = bb[p * L + l] * rate + sum_bar;
+            const double B = c.bwid[p * L + l], n = c.bman[p * L + l];
+            const double h_si = hs[l];
+            const double qq = in[6 + l] / B;
+            const double inv = 1.0 / (h_si * h_si * cbrt(h_si));
+            const double drive = qq + gdt * h_si * slope;
+            const double drag = 1.0 + gdt * (n * n) * fabs(qq) * inv;
+            const double out = B * drive / drag;
+            const double drive_bar = q_bar / drag * B;
+            const double drag_bar = -q_bar * out / drag;
+            double qq_bar = drive_bar + drag_bar * gdt * (n * n) * (double)((qq > 0.0) - (qq < 0.0)) * inv;
+            const double inv_bar = drag_bar * gdt * (n * n) * fabs(qq);
+            double hsi_bar = drive_bar * gdt * slope + inv_bar * (-(7.0 / 3.0) * inv / h_si);
+            slope_bar += drive_bar * gdt * h_si;
+            flux_bar[l] = qq_bar / B;
+            // semi-implicit depth
+            if (c.lev) {
+                if (l == 0) {
+                    const double d0 = in[6 + L];
+                    const double r = sqrt(h[l] * d0);
+                    if (r > 0.0) {
+                        const double arg_bar = hsi_bar / (2.0 * r);
+                        h_bar += arg_bar * d0;
+                        depth_bar[0] += arg_bar * h[l];
+                    } else {
+                        h_bar += hsi_bar;
+                    }
+                } else {
+                    h_bar += hsi_bar;
+                }
+            } else {
+                const double d = in[6 + L + l];
+                const double r1 = sqrt(h[l] * d), r2 = sqrt(h[l] * 0.01);
+                if (r1 >= r2) {
+                    if (h[l] * d > 0.0) {
+                        const double arg_bar = hsi_bar / (2.0 * r1);
+                        h_bar += arg_bar * d;
+                        depth_bar[l] += arg_bar * h[l];
+                    }
+                } else if (h[l] * 0.01 > 0.0) {
+                    h_bar += hsi_bar / (2.0 * r2) * 0.01;
+                }
+            }
+        }
+        if (hpos[l]) {
+            if (c.lev && l > 0) ptop_bar += h_bar;
+            else top_bar += h_bar;
+        }
+    }
+
+    // end states
+    double in_bar[6] = {0.0, 0.0, 0.0, 0.0, st_a_bar, st_b_bar};
+    if (top_a) in_bar[0] += top_bar;
+    else in_bar[1] += top_bar;
+    if (c.lev) {
+        if (ptop_a) in_bar[2] += ptop_bar;
+        else in_bar[3] += ptop_bar;
+    } else {
+        if (top_a) in_bar[0] += ptop_bar;
+        else in_bar[1] += ptop_bar;
+    }
+    if (slope_free) {
+        in_bar[0] += slope_bar / len;
+        in_bar[1] -= slope_bar / len;
+    }
+
+    // write, as the dual-number form does
+    for (int l = 0; l < L; ++l) {
+        lam_path(c, a.lam, PF_BOUT)[p * L + l] = flux_bar[l];
+        lam_path(c, a.lam, PF_BCSD)[p * L + l] = depth_bar[l];
+    }
+    for (int end = 0; end < 2; ++end) {
+        double* qe = peb(c, a.scr) + 8L * p + 4 * end;
+        qe[0] = in_bar[end];
+        const double v = in_bar[2 + end];
+        const int e = end ? di : ci;
+        bool to_pdep = false;
+        if (c.lev && (c.flags[e] & CMF_CELL_LEVEE)) {
+            const double wse = X[F_RDEP * N + e] + (c.celv[e] - c.rh[e]);
+            to_pdep = c.celv[e] + X[F_PDEP * N + e] <= wse;
+        }
+        qe[1] = to_pdep ? 0.0 : v;
+        qe[2] = to_pdep ? v : 0.0;
+        qe[3] = in_bar[4 + end];
+    }
+}
+
+__host__ __device__ constexpr int path_reverse_threads(long, int L)
+{
+    return CMF_ADJ_PATH_HAND ? 1 : path_threads(L);
+}
+
 // Momentum reversed (kr_momentum): lambda_k of the cell, the downstream-depth
 // adjoint left for the downstream cell, parameter gradients.
 __device__ __forceinline__ void dam_reverse(const Ctx& c, const double* X, const double* runoff,
@@ -1202,8 +1404,11 @@ __global__ void __launch_bounds__(kBlock, CMF_ADJ_MIN_BLOCKS) kr_momentum(const 
     if ((int)blockIdx.x >= c.grid_cells) {
         // trailing blocks: path direction threads, then dam direction threads
         const long b = (long)blockIdx.x - c.grid_cells;
-        const long pb = c.bif ? (c.P * path_threads(c.L) + kBlock - 1) / kBlock : 0;
-        if (b < pb) path_reverse(c, X, dt, a, b * blockDim.x + threadIdx.x);
+        const long pb = c.bif ? (c.P * path_reverse_threads(c.P, c.L) + kBlock - 1) / kBlock : 0;
+        if (b < pb) {
+            if (CMF_ADJ_PATH_HAND) path_reverse_hand(c, X, dt, a, b * blockDim.x + threadIdx.x);
+            else path_reverse(c, X, dt, a, b * blockDim.x + threadIdx.x);
+        }
         else dam_reverse(c, X, runoff, dt, a, (b - pb) * blockDim.x + threadIdx.x);
         return;
     }
@@ -1650,7 +1855,7 @@ int cmf_adj_reverse(CmfAdjPlan* plan, void* stream, const double* tape, int num_
         if (c.bif) launch_dep(kr_stage_path, c.grid_paths, s, c, X, a);
         launch_dep(kr_limit, c.grid_cells, s, c, X, dt, a);
         // cells, then the path and dam direction threads in trailing blocks
-        const int path_blocks = c.bif ? (int)((c.P * path_threads(c.L) + kBlock - 1) / kBlock) : 0;
+        const int path_blocks = c.bif ? (int)((c.P * path_reverse_threads(c.P, c.L) + kBlock - 1) / kBlock) : 0;
         const int dam_blocks = (c.res && c.ND > 0) ? (int)((c.ND * kDamDirs + kBlock - 1) / kBlock) : 0;
         launch_dep(kr_momentum, c.grid_cells + path_blocks + dam_blocks, s, c, X, runoff, dt, a);
     }
