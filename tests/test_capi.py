@@ -48,3 +48,7 @@ def test_workspace_size_and_argument_errors():
     v.abi_version = 999
     assert h.cmf_plan_create(ctypes.byref(v), ctypes.byref(plan)) == _lib.CMF_ERR_ARG
     assert h.cmf_step_interval(None, None, 86400.0, 0) == _lib.CMF_ERR_ARG
+    # the plan setters refuse a null plan without touching a device
+    assert h.cmf_plan_set_persistent(None, 1) == _lib.CMF_ERR_ARG
+    assert h.cmf_plan_set_persistent(None, 0) == _lib.CMF_ERR_ARG
+    assert h.cmf_plan_set_member_tile(None, 2) == _lib.CMF_ERR_ARG
