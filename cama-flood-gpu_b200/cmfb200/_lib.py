@@ -172,6 +172,8 @@ def lib() -> ctypes.CDLL:
     h.cmf_plan_set_member_tile.argtypes = [_P, _I32]
     h.cmf_plan_set_persistent.restype = ctypes.c_int
     h.cmf_plan_set_persistent.argtypes = [_P, ctypes.c_int]
+    h.cmf_probe_barrier_timeout.restype = ctypes.c_int
+    h.cmf_probe_barrier_timeout.argtypes = [_P, _P, _P, _I32]
     h.cmf_step_interval.restype = ctypes.c_int
     h.cmf_step_interval.argtypes = [_P, _P, _F64, _I32]
     h.cmf_phase_momentum.restype = ctypes.c_int

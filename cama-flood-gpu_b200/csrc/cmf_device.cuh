@@ -959,11 +959,13 @@ __device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned lo
 }
 
 // false: the interval was abandoned (a barrier gave up); the caller returns.
-__device__ __forceinline__ bool grid_barrier(int* ctl, int* status, unsigned long long& target)
+__device__ __forceinline__ bool grid_barrier(int* ctl, int* status, unsigned long long& target,
+                                             unsigned long long timeout_ns = kBarrierTimeoutNs,
+                                             unsigned arrivals = 0)
 {
     __shared__ int go_on;
     __syncthreads();
-    target += gridDim.x;
+    target += arrivals ? arrivals : gridDim.x;
     if (threadIdx.x == 0) {
         unsigned long long* count = reinterpret_cast<unsigned long long*>(ctl + kCtlBarrier);
         volatile int* abort_flag = ctl + kCtlAbort;
@@ -973,7 +975,7 @@ __device__ __forceinline__ bool grid_barrier(int* ctl, int* status, unsigned lon
         const unsigned long long t0 = global_ns();
         while (load_acquire_u64(count) < target) {
             if (*abort_flag) { ok = 0; break; }
-            if (global_ns() - t0 > kBarrierTimeoutNs) {
+            if (global_ns() - t0 > timeout_ns) {
                 atomicOr(status, CMF_STATUS_SYNC_TIMEOUT);
                 atomicExch(ctl + kCtlAbort, 1);
                 ok = 0;
@@ -1015,6 +1017,16 @@ __global__ void __launch_bounds__(256, CMF_PERSIST_MIN_BLOCKS) k_persistent(cons
         }
     }
     if (first == 0) v.ctl[kCtlStep] = n;
+}
+
+// The barrier's give-up path, for a test: every block arrives once at a
+// barrier that waits for one arrival more than the grid has, so each wait
+// runs out after timeout_ns, raises CMF_STATUS_SYNC_TIMEOUT and the abort
+// flag, and the kernel returns.
+__global__ void k_barrier_timeout_probe(int* ctl, int* status, unsigned long long timeout_ns)
+{
+    unsigned long long target = 0;
+    grid_barrier(ctl, status, target, timeout_ns, gridDim.x + 1);
 }
 
 // ---------------------------------------------------------------------------

@@ -904,6 +904,18 @@ int cmf_plan_set_persistent(CmfPlan* p, int enable)
     return CMF_OK;
 }
 
+int cmf_probe_barrier_timeout(void* stream, int32_t* control, int32_t* status, int32_t timeout_us)
+{
+    if (!control || !status || timeout_us <= 0 || timeout_us > 1000000) return CMF_ERR_ARG;
+    if (((uintptr_t)control & 7) != 0) return CMF_ERR_ARG;
+    int* ctl = control;
+    int* st = status;
+    unsigned long long ns = (unsigned long long)timeout_us * 1000ull;
+    void* args[] = {&ctl, &st, &ns};
+    return check_cuda(cudaLaunchCooperativeKernel((const void*)k_barrier_timeout_probe, dim3(2), dim3(32),
+                                                  args, 0, (cudaStream_t)stream));
+}
+
 int cmf_plan_set_member_tile(CmfPlan* p, int32_t width)
 {
     if (!p || width < 1) return CMF_ERR_ARG;

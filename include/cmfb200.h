@@ -236,6 +236,13 @@ void cmf_plan_destroy(CmfPlan* plan);
  * CMF_STATUS_SYNC_TIMEOUT and ends the interval.  enable == 0 returns to the
  * interval graph. */
 int cmf_plan_set_persistent(CmfPlan* plan, int enable);
+/* Test of the persistent kernel's failure path (no counterpart in the
+ * reference): launches, cooperatively, two blocks that meet at a grid barrier
+ * waiting for one arrival more than they make, so each wait gives up after
+ * timeout_us (1 .. 1,000,000), sets CMF_STATUS_SYNC_TIMEOUT in *status and
+ * the abort word in control[6], and returns; nothing hangs.  control: 16
+ * device int32 words, zeroed by the caller, 8-byte aligned. */
+int cmf_probe_barrier_timeout(void* stream, int32_t* control, int32_t* status, int32_t timeout_us);
 /* Member-tile width of the member-batched kernels (no counterpart in the
  * reference): each thread handles `width` consecutive members of one
  * catchment, so the catchment's shared fields are loaded once from HBM and

@@ -52,3 +52,4 @@ def test_workspace_size_and_argument_errors():
     assert h.cmf_plan_set_persistent(None, 1) == _lib.CMF_ERR_ARG
     assert h.cmf_plan_set_persistent(None, 0) == _lib.CMF_ERR_ARG
     assert h.cmf_plan_set_member_tile(None, 2) == _lib.CMF_ERR_ARG
+    assert h.cmf_probe_barrier_timeout(None, None, None, 10) == _lib.CMF_ERR_ARG

@@ -89,3 +89,26 @@ def test_persistent_refuses_what_it_does_not_run(device):
     rf = np.ones((net.num_catchments, 2), dtype=np.float32)
     with pytest.raises(ValueError):
         P.model_for(net, num_members=2, batched_fields={"river_manning": rf}, persistent=True)
+
+
+def test_barrier_wait_gives_up_and_reports(device):
+    """The persistent kernel's barrier is bounded: a barrier that waits for
+    one arrival more than the grid makes (a count nothing completes) gives up
+    after its time limit, reports CMF_STATUS_SYNC_TIMEOUT and the abort word,
+    and the kernel returns; the context stays usable."""
+    import time
+    from cmfb200 import _lib
+    ctl = torch.zeros(16, dtype=torch.int32, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    t0 = time.perf_counter()
+    rc = _lib.lib().cmf_probe_barrier_timeout(stream, ctl.data_ptr(), status.data_ptr(), 20000)
+    assert rc == _lib.CMF_OK
+    torch.cuda.synchronize(device)
+    assert time.perf_counter() - t0 < 10.0
+    assert int(status.item()) & _lib.STATUS_SYNC_TIMEOUT
+    c = ctl.cpu().numpy()
+    assert c[6] == 1                                    # abort word
+    assert int(c[4]) + (int(c[5]) << 32) == 2           # both blocks arrived once
+    x = torch.arange(100, device=device, dtype=torch.float32)
+    assert float(x.sum().item()) == 4950.0
