@@ -367,6 +367,19 @@ def statistics_overhead(model, dev_forcing, first: int, steps: int, base_ms: flo
             "sub_steps": sub, "finite": ok}
 
 
+ENSEMBLE_CHECK_FIELDS = ("river_storage", "flood_storage", "river_outflow", "flood_outflow",
+                         "river_depth", "flood_depth", "flood_fraction")
+
+
+def _bit_sums(t):
+    """Sum over catchments of the integer bit patterns of a state field
+    ([N] -> scalar, [N, M] -> [M]): equal states give equal sums, and a single
+    differing bit changes them."""
+    import torch
+    as_int = t.contiguous().view(torch.int64 if t.element_size() == 8 else torch.int32)
+    return as_int.to(torch.int64).sum(dim=0)
+
+
 def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
                      member_tile: int = 16, block: int = 64, days: int = 5) -> dict:
     """The batched-ensemble workload: `members` members of a `basins`-basin
@@ -379,7 +392,9 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
     `member_tile` members of a catchment per thread in CTAs of `block` threads
     (member_tile 0: the autotuner picks both on the first day); the looped
     plain models keep their default CTA size.  Forcing of every day and member
-    is resident on the device before timing."""
+    is resident on the device before timing.  Each member's end state is
+    checked against its looped run (bit-pattern sums of seven state fields;
+    the looped fingerprints are timed apart and left out of the looped time)."""
     import torch
     from cmfb200 import CaMaFlood, synthetic as syn
     net = syn.generate_basins(basins, catchments, seed=3)
@@ -421,6 +436,8 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
     t_batched = a.elapsed_time(b) / 1e3
     n_batched = int(cnt_b.sum().item())
     tile, block = ens.member_tile, ens.block_size
+    # each member's end state, as integer sums of the bit patterns of its fields
+    fp_b = torch.stack([_bit_sums(getattr(ens.base, k)) for k in ENSEMBLE_CHECK_FIELDS])  # [F, M]
     ens.close()
     del ens, init, forcing
 
@@ -434,6 +451,9 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
     torch.cuda.synchronize(device)
     a.record(stream)
     cnt_l = torch.zeros((members, days), dtype=torch.int32, device=device)
+    fp_l = torch.zeros((len(ENSEMBLE_CHECK_FIELDS), members), dtype=torch.int64, device=device)
+    f_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(members)]
     for m in range(members):
         reset(plain, init)
         plain.base.river_manning.copy_(man_dev[m])
@@ -441,9 +461,15 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
             plain.set_inputs(run_dev[m, d])
             plain.step_advance()
             cnt_l[m, d].copy_(plain.sub_step_counts()[0])
+        f_ev[m][0].record(stream)
+        for j, k in enumerate(ENSEMBLE_CHECK_FIELDS):
+            fp_l[j, m] = _bit_sums(getattr(plain.base, k))
+        f_ev[m][1].record(stream)
     b.record(stream)
     torch.cuda.synchronize(device)
-    t_looped = a.elapsed_time(b) / 1e3
+    # the end-state fingerprints are not part of the looped runs' time
+    t_looped = (a.elapsed_time(b) - sum(e0.elapsed_time(e1) for e0, e1 in f_ev)) / 1e3
+    state_equal = bool(torch.equal(fp_b, fp_l))
     n_looped = int(cnt_l.sum().item())
     same_counts = bool(torch.equal(cnt_b, cnt_l.T))
     plain.close()
@@ -468,6 +494,8 @@ def ensemble_compare(device, members: int, catchments: int, basins: int = 500,
             "member_tile": tile, "block": block, "days": days,
             "sub_steps_per_member_mean": n_batched / members,
             "same_sub_step_counts": same_counts,
+            "members_equal_looped_runs": state_equal,
+            "checked_fields": list(ENSEMBLE_CHECK_FIELDS),
             "workload": f"{days} days (a sample of the 30-day window) of a member-innermost "
                         "ensemble (runoff x lognormal(0.3), river Manning x U(0.8,1.2) per member) "
                         "vs the members looped as plain models over the same days; includes the "
