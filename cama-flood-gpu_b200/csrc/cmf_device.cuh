@@ -831,12 +831,16 @@ __device__ __forceinline__ void levee_cell(const Dev<REAL>& v, long li, int m, i
     double* fdst = (k & 1) ? v.fs0 : v.fs1;
     const long ci = v.lci[li];
     const long cm = ix<ONE>(ci, m, v.M);
+    // The cell's river and flood storage decide the regime; its depths and
+    // flooded fraction are read only where a regime uses them (the flood
+    // depth when overtopped) and written only where a regime changes them:
+    // the scattered levee cells cost a sector per field touched.
     LeveeState<double, REAL> lst;
     lst.rs = rdst[cm];
     lst.fs = fdst[cm];
-    lst.rdep = v.rdep[cm];
-    lst.fdep = v.fdep[cm];
-    lst.ffr = v.ffr[cm];
+    lst.rdep = REAL(0);
+    lst.fdep = REAL(0);
+    lst.ffr = REAL(0);
     // static fields from the levee-indexed copies where the plan keeps
     // them (coalesced over the levee list), else from the cells
     const REAL* row = v.lpk_tbl ? v.lpk_tbl + li * (long)v.K : v.tbl + ci * (long)v.K;
@@ -852,6 +856,7 @@ __device__ __forceinline__ void levee_cell(const Dev<REAL>& v, long li, int m, i
         rl = par<ONE>(v.rl, CMF_BATCH_RIVER_LENGTH, v.batched, ci, m, v.M);
     }
     const REAL crown = v.lcrown[li], frac = v.lfrac[li], base = v.lbase[li];
+    int regime;
     if (v.lmk) {
         // the plan's marks: the row is read only while the protected
         // side fills
@@ -863,17 +868,26 @@ __device__ __forceinline__ void levee_cell(const Dev<REAL>& v, long li, int m, i
         mk.s_first = v.lmk[3 * n + li];
         mk.dw = v.lmk[4 * n + li];
         mk.dist = v.lmk[5 * n + li];
-        levee_apply<0>(lst, mk, rw, rh, rl, crown, frac, base, v.K, depth);
+        // the overtopped test of levee_apply, to fetch the flood depth it reads
+        const REAL total = narrow<REAL>(lst.rs + lst.fs);
+        const REAL bank = xmul(xmul(rl, rw), rh);
+        if (total >= bank && total >= mk.s_crown) lst.fdep = v.fdep[cm];
+        regime = levee_apply<0>(lst, mk, rw, rh, rl, crown, frac, base, v.K, depth);
     } else {
-        levee_partition<0>(lst, rw, rh, rl, v.ca[ci], crown, frac, base, v.K, depth);
+        lst.fdep = v.fdep[cm];
+        regime = levee_partition<0>(lst, rw, rh, rl, v.ca[ci], crown, frac, base, v.K, depth);
     }
-    rdst[cm] = lst.rs;
-    fdst[cm] = lst.fs;
     v.ps[cm] = lst.ps;
-    v.rdep[cm] = lst.rdep;
-    v.fdep[cm] = lst.fdep;
     v.pdep[cm] = lst.pdep;
-    v.ffr[cm] = lst.ffr;
+    if (regime == kLeveeOvertopped) {
+        fdst[cm] = lst.fs;
+    } else if (regime == kLeveeFilling || regime == kLeveeWedge) {
+        rdst[cm] = lst.rs;
+        fdst[cm] = lst.fs;
+        v.rdep[cm] = lst.rdep;
+        v.fdep[cm] = lst.fdep;
+        v.ffr[cm] = lst.ffr;
+    }
 }
 
 template <typename REAL, bool ONE>

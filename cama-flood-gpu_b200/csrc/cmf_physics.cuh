@@ -378,6 +378,18 @@ __device__ __forceinline__ StageOut<S, R> flood_stage_of(S S_tot, R width, R len
 // the river geometry (width, height), P static inputs (length, area, levee
 // parameters, table depths).
 // ---------------------------------------------------------------------------
+// Which regime a levee partition took; a caller that keeps the cell's fields
+// in memory stores only what that regime changed (river storage, depths and
+// flooded fraction pass through unchanged below the banks, below the levee
+// base and when overtopped; the flood storage also below the base).
+enum LeveeRegime : int {
+    kLeveeBelowBank = 0,  // sets ps, pdep
+    kLeveeOvertopped,     // sets fs, ps, pdep (reads rs, fs, fdep)
+    kLeveeFilling,        // sets every field
+    kLeveeWedge,          // sets every field
+    kLeveeNoEffect,       // sets ps, pdep
+};
+
 template <typename S, typename R>
 struct LeveeState {
     S rs, fs, ps;            // river / flood / protected storage
@@ -548,7 +560,7 @@ __device__ __forceinline__ ProtectedFill<G, P> protected_fill(V total, G bank, G
 // The partition itself, on the levee's marks; the floodplain row is read
 // only when the protected side is filling.
 template <int KR, typename S, typename R, typename G, typename P, typename Depth>
-__device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMarks<G, P>& mk,
+__device__ __forceinline__ int levee_apply(LeveeState<S, R>& st, const LeveeMarks<G, P>& mk,
                                             G width, G height, P len, P crown, P frac, P base,
                                             int K, Depth depth_at)
 {
@@ -559,7 +571,7 @@ __device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMar
     if (!(val(total) >= val(bank))) {
         st.ps = S(0);
         st.pdep = R(0);
-        return;
+        return kLeveeBelowBank;
     }
     const G wedge = xadd(G(mk.dist), width);
     if (val(total) >= val(mk.s_crown)) {
@@ -572,7 +584,7 @@ __device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMar
         st.ps = pos_part(remaining - fs);
         st.fs = fs;
         st.pdep = st.fdep;
-        return;
+        return kLeveeOvertopped;
     }
     if (val(total) >= val(mk.s_top)) {
         // river side at the crown, the protected side filling
@@ -605,7 +617,7 @@ __device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMar
         st.fdep = R(crown);
         st.pdep = pdep;
         st.ffr = smin(smax(pfrac, R(0)), R(1));
-        return;
+        return kLeveeFilling;
     }
     if (val(total) >= val(mk.s_base)) {
         // water rising in the wedge between the river and the levee
@@ -620,18 +632,19 @@ __device__ __forceinline__ void levee_apply(LeveeState<S, R>& st, const LeveeMar
         st.fdep = fdep;
         st.pdep = R(0);
         st.ffr = R(frac);
-        return;
+        return kLeveeWedge;
     }
     // below the levee base: no levee effect
     const S remaining = pos_part(total_s - st.rs);
     st.ps = pos_part(remaining - st.fs);
     st.pdep = R(0);
+    return kLeveeNoEffect;
 }
 
 // Marks and partition in one call (geometry that varies by member, the
 // adjoint).  A cell below its banks needs neither.
 template <int KR, typename S, typename R, typename G, typename P, typename Depth>
-__device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G height, P len,
+__device__ __forceinline__ int levee_partition(LeveeState<S, R>& st, G width, G height, P len,
                                                 P area, P crown, P frac, P base, int K,
                                                 Depth depth_at)
 {
@@ -640,11 +653,11 @@ __device__ __forceinline__ void levee_partition(LeveeState<S, R>& st, G width, G
     if (!(val(total) >= val(bank))) {
         st.ps = S(0);
         st.pdep = R(0);
-        return;
+        return kLeveeBelowBank;
     }
     const LeveeMarks<G, P> mk =
         levee_marks_of<KR>(width, height, len, area, crown, frac, base, K, depth_at);
-    levee_apply<KR>(st, mk, width, height, len, crown, frac, base, K, depth_at);
+    return levee_apply<KR>(st, mk, width, height, len, crown, frac, base, K, depth_at);
 }
 
 }  // namespace cmf
