@@ -48,9 +48,16 @@
 #ifndef CMF_PERSIST_MIN_BLOCKS
 #define CMF_PERSIST_MIN_BLOCKS 4
 #endif
+// k_stage: 5 CTAs (48 registers) for one fp32 member, which walks the
+// floodplain row from memory (L1) instead of holding it in registers (234 ->
+// 223 us per 6M sub-step); 4 CTAs (64 registers, the row in registers) for
+// fp64 and for member-batched runs
 #ifndef CMF_STAGE_MIN_BLOCKS
-#define CMF_STAGE_MIN_BLOCKS 4
+#define CMF_STAGE_MIN_BLOCKS(REAL, ONE) ((sizeof(REAL) == 4 && (ONE)) ? 5 : 4)
 #endif
+// whether a k_stage instantiation holds the floodplain row in registers
+template <typename REAL, bool ONE>
+__host__ __device__ constexpr bool stage_row_in_regs() { return !(sizeof(REAL) == 4 && ONE); }
 // k_momentum: 8 CTAs (32 registers) for one fp32 member, where the few bytes
 // it spills cost less than the occupancy they buy (182 -> 161 us per 6M
 // sub-step); fp64 and member-batched variants would spill hundreds of bytes
@@ -538,8 +545,11 @@ __device__ __forceinline__ REAL limit_rate_of(const Dev<REAL>& v, const double* 
 // early for cells that were flooded before the sub-step.  Other level counts
 // walk the row in memory.
 // ---------------------------------------------------------------------------
-template <typename REAL>
+template <typename REAL, bool REGS = true>
 struct CellProfile {
+    // REGS: the CaMa row (kRowRegs levels) is held in registers; otherwise
+    // every level count walks the row in memory
+    static constexpr bool kRegs = REGS;
     const Dev<REAL>* v;
     long i;
     REAL D[kRowRegs];
@@ -564,7 +574,7 @@ struct CellProfile {
         ca = v->ca[i];
         loaded = true;
     }
-    __device__ bool in_regs() const { return v->K == kRowRegs; }
+    __device__ bool in_regs() const { return REGS && v->K == kRowRegs; }
     __device__ REAL area()
     {
         if (!in_regs()) return v->ca[i];
@@ -650,11 +660,11 @@ __device__ __forceinline__ void stage_cell(const Dev<REAL>& v, long i, int m, in
 
     // A cell flooded in the previous sub-step will almost surely need its
     // floodplain row: start those loads now, alongside the upstream gather.
-    CellProfile<REAL> prof;
+    CellProfile<REAL, stage_row_in_regs<REAL, ONE>()> prof;
     prof.v = &v;
     prof.i = i;
     prof.loaded = false;
-    if (v.K == kRowRegs && fsto > 0.0) prof.load();
+    if (prof.in_regs() && fsto > 0.0) prof.load();
 
     // upstream inflow: gather the limited fluxes of the upstream cells, in
     // range order, child_unroll independent loads at a time
@@ -907,7 +917,7 @@ __global__ void __launch_bounds__(256) k_levee(const Dev<REAL> v, int kh, int fo
 }
 
 template <typename REAL, bool ONE, bool RES, bool LEV, bool BIF, bool BUDGET>
-__global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS) k_stage(const Dev<REAL> v, int kh, int force_diag,
+__global__ void __launch_bounds__(256, CMF_STAGE_MIN_BLOCKS(REAL, ONE)) k_stage(const Dev<REAL> v, int kh, int force_diag,
                                                cudaGraphConditionalHandle h, int set_cond)
 {
     const int W = mtile_of<REAL, ONE>(v);
