@@ -540,10 +540,11 @@ __device__ __forceinline__ REAL limit_rate_of(const Dev<REAL>& v, const double* 
 
 // ---------------------------------------------------------------------------
 // A catchment's floodplain profile for the flood stage: the catchment area
-// and the table row, needed only by cells above their banks.  The CaMa layout
-// (kRowRegs levels) keeps the row in registers; stage_cell starts its loads
-// early for cells that were flooded before the sub-step.  Other level counts
-// walk the row in memory.
+// and the table row, needed only by cells above their banks.  With REGS and
+// the CaMa layout (kRowRegs levels) the row is held in registers and
+// stage_cell starts its loads early for cells that were flooded before the
+// sub-step; otherwise the walk reads the row from memory (L1) level by level,
+// which leaves the single-member fp32 stage room for more resident CTAs.
 // ---------------------------------------------------------------------------
 template <typename REAL, bool REGS = true>
 struct CellProfile {
